@@ -1,0 +1,282 @@
+"""ctypes binding of libcfdgpu.so (the C ABI in include/cfdgpu.h and
+include/cfdgpu_host.h).
+
+The Solver class follows the reference's plugin contract
+(euler_equations/euler_simulation_code/headers/problem_base.hpp:18-40 and
+headers/simulation.hpp:36-67): upload the initial grid, then per step
+``compute_dt`` followed by ``step``; ``advance`` runs the same loop on the
+device.  There is no CPU fallback: constructing a Solver without the built
+library or without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libcfdgpu.so"
+
+EULER, ALLAIRE = 0, 1
+FP64, MIXED = 0, 1
+TRANSMISSIVE, REFLECTIVE = 0, 1
+LIMITERS = {"minmod": 0, "vanleer": 1, "mc": 2, "unlimited": 3}
+FLUX = {"MUSCL": 0, "Godunov": 1}
+SPLIT = {"naive": 0, "strang": 1}
+WAVESPEED = {"davis": 0, "pvrs": 1}
+GHOSTED_AOS, SOA = 0, 1
+RECIPE = {"four_quadrant": 1, "shock_bubbles": 2, "water_shock_air_bubble": 3}
+COUNTERS = ["unphysical_input", "slope_zeroed", "first_order", "fixup", "unphysical_output"]
+
+
+class CfdError(RuntimeError):
+    pass
+
+
+class Config(C.Structure):
+    """Mirror of ``cfd_config``."""
+
+    _fields_ = [
+        ("model", C.c_int), ("precision", C.c_int), ("nx", C.c_int), ("ny", C.c_int),
+        ("x0", C.c_double), ("y0", C.c_double), ("dx", C.c_double), ("dy", C.c_double),
+        ("gamma1", C.c_double), ("pinf1", C.c_double), ("gamma2", C.c_double),
+        ("pinf2", C.c_double), ("bc", C.c_int * 4), ("cfl", C.c_double), ("T", C.c_double),
+        ("limiter", C.c_int), ("flux_solver", C.c_int), ("splitting", C.c_int),
+        ("wavespeed", C.c_int), ("z_min", C.c_double), ("fix_dy_halfstep", C.c_int),
+        ("stream", C.c_void_p),
+    ]
+
+    @property
+    def nvar(self) -> int:
+        return 4 if self.model == EULER else 6
+
+    @property
+    def ghosts(self) -> int:
+        return 1 if self.flux_solver == FLUX["Godunov"] else 2
+
+    def ghosted_shape(self) -> tuple[int, int, int]:
+        g = self.ghosts
+        return (self.ny + 2 * g, self.nx + 2 * g, self.nvar)
+
+    def copy(self) -> "Config":
+        c = Config()
+        C.pointer(c)[0] = self
+        return c
+
+
+class Status(C.Structure):
+    _fields_ = [
+        ("n", C.c_int), ("done", C.c_int), ("t", C.c_double), ("dt_next", C.c_double),
+        ("maxu", C.c_double), ("maxv", C.c_double), ("mass1", C.c_double), ("mass2", C.c_double),
+        ("counters", C.c_ulonglong * 8),
+    ]
+
+    def counter_dict(self) -> dict[str, int]:
+        return {k: int(self.counters[i]) for i, k in enumerate(COUNTERS)}
+
+
+_lib: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    """Loads libcfdgpu.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise CfdError(f"{LIB_PATH} not built (run cfd-art_b200/build.py)")
+        L = C.CDLL(str(LIB_PATH))
+        vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.c_int
+        cfgp = C.POINTER(Config)
+        sig = {
+            "cfd_version": (C.c_char_p, []),
+            "cfd_last_error": (ip, [C.c_char_p, C.c_size_t]),
+            "cfd_nvar": (ip, [ip]),
+            "cfd_device_bytes": (ip, [cfgp, C.POINTER(C.c_size_t)]),
+            "cfd_create": (ip, [cfgp, C.POINTER(vp)]),
+            "cfd_destroy": (ip, [vp]),
+            "cfd_upload": (ip, [vp, dp, ip, ip, C.c_double]),
+            "cfd_upload_device": (ip, [vp, vp, ip, C.c_double]),
+            "cfd_download": (ip, [vp, dp, ip]),
+            "cfd_compute_dt": (ip, [vp, ip, C.c_double, dp]),
+            "cfd_step": (ip, [vp, C.c_double]),
+            "cfd_advance": (ip, [vp, ip]),
+            "cfd_get_status": (ip, [vp, C.POINTER(Status)]),
+            "cfd_reset_counters": (ip, [vp]),
+            "cfd_set_kernel_timing": (ip, [vp, ip]),
+            "cfd_kernel_times": (ip, [vp, dp, C.POINTER(ip)]),
+            "cfd_reset_kernel_times": (ip, [vp]),
+            "cfd_synchronize": (ip, [vp]),
+            "cfd_state_device": (ip, [vp, C.POINTER(vp), C.POINTER(C.c_int64), C.POINTER(ip)]),
+            "cfd_face_flux": (ip, [cfgp, ip, dp, C.c_double, C.c_double, dp, dp, dp]),
+            "cfd_ic_grid_elems": (ip, [cfgp, C.POINTER(C.c_size_t)]),
+            "cfd_case_config": (ip, [ip, C.c_char_p, ip, ip, ip, cfgp]),
+            "cfd_case_ic": (ip, [cfgp, C.c_char_p, C.c_uint64, dp]),
+            "cfd_recipe_config": (ip, [ip, ip, ip, cfgp]),
+            "cfd_recipe_ic": (ip, [cfgp, ip, C.c_uint64, ip, dp]),
+            "cfd_write_state": (ip, [cfgp, dp, C.c_char_p, C.c_double]),
+            "cfd_write_schlieren": (ip, [cfgp, dp, C.c_char_p, C.c_double]),
+            "cfd_write_masschange": (ip, [cfgp, C.c_char_p, ip, dp, dp, dp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().cfd_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != 0:
+        raise CfdError(f"{what} failed ({rc}): {last_error()}")
+
+
+def _dp(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise ValueError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def case_config(model: int, test_case: str, nx: int, ny: int, flux_solver: str = "MUSCL") -> Config:
+    cfg = Config()
+    check(lib().cfd_case_config(model, test_case.encode(), nx, ny, FLUX[flux_solver],
+                                C.byref(cfg)), f"case_config({test_case})")
+    return cfg
+
+
+def case_ic(cfg: Config, test_case: str, seed: int = 0) -> np.ndarray:
+    grid = np.zeros(cfg.ghosted_shape())
+    check(lib().cfd_case_ic(C.byref(cfg), test_case.encode(), seed, _dp(grid)),
+          f"case_ic({test_case})")
+    return grid
+
+
+def recipe_config(name: str, nx: int, ny: int) -> Config:
+    cfg = Config()
+    check(lib().cfd_recipe_config(RECIPE[name], nx, ny, C.byref(cfg)), f"recipe_config({name})")
+    return cfg
+
+
+def recipe_ic(cfg: Config, name: str, seed: int = 20261203, nbubbles: int = 32) -> np.ndarray:
+    grid = np.zeros(cfg.ghosted_shape())
+    check(lib().cfd_recipe_ic(C.byref(cfg), RECIPE[name], seed, nbubbles, _dp(grid)),
+          f"recipe_ic({name})")
+    return grid
+
+
+def face_flux(cfg: Config, stencils: np.ndarray, dt: float, dx: float):
+    """Device flux of independent faces: stencils (nfaces, 4|2, nvar)."""
+    st = np.ascontiguousarray(stencils, dtype=np.float64)
+    nf = st.shape[0]
+    nv = cfg.nvar
+    flux = np.zeros((nf, nv))
+    us = np.zeros(nf)
+    zs = np.zeros(nf)
+    check(lib().cfd_face_flux(C.byref(cfg), nf, _dp(st), dt, dx, _dp(flux), _dp(us), _dp(zs)),
+          "face_flux")
+    return flux, us, (zs if cfg.model == ALLAIRE else None)
+
+
+class Solver:
+    """One device-resident solve (cfd_create ... cfd_destroy)."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg.copy()
+        h = C.c_void_p()
+        check(lib().cfd_create(C.byref(self.cfg), C.byref(h)), "cfd_create")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().cfd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, grid: np.ndarray, n: int = 0, t: float = 0.0, layout: int = GHOSTED_AOS):
+        check(lib().cfd_upload(self._h, _dp(grid), layout, n, t), "cfd_upload")
+
+    def upload_device(self, ptr: int, n: int = 0, t: float = 0.0):
+        check(lib().cfd_upload_device(self._h, C.c_void_p(ptr), n, t), "cfd_upload_device")
+
+    def download(self, layout: int = GHOSTED_AOS, out: np.ndarray | None = None) -> np.ndarray:
+        c = self.cfg
+        if out is None:
+            shape = c.ghosted_shape() if layout == GHOSTED_AOS else (c.nvar, c.ny, c.nx)
+            out = np.empty(shape)
+        check(lib().cfd_download(self._h, _dp(out), layout), "cfd_download")
+        return out
+
+    def compute_dt(self, n: int, t: float) -> float:
+        dt = C.c_double()
+        check(lib().cfd_compute_dt(self._h, n, t, C.byref(dt)), "cfd_compute_dt")
+        return dt.value
+
+    def step(self, dt: float) -> None:
+        check(lib().cfd_step(self._h, dt), "cfd_step")
+
+    def advance(self, max_steps: int) -> None:
+        check(lib().cfd_advance(self._h, max_steps), "cfd_advance")
+
+    def status(self) -> Status:
+        st = Status()
+        check(lib().cfd_get_status(self._h, C.byref(st)), "cfd_get_status")
+        return st
+
+    def set_kernel_timing(self, on: bool) -> None:
+        check(lib().cfd_set_kernel_timing(self._h, int(on)), "cfd_set_kernel_timing")
+
+    def kernel_times(self):
+        ms = (C.c_double * 2)()
+        n = (C.c_int * 2)()
+        check(lib().cfd_kernel_times(self._h, ms, n), "cfd_kernel_times")
+        return [ms[0], ms[1]], [n[0], n[1]]
+
+    def reset_kernel_times(self) -> None:
+        check(lib().cfd_reset_kernel_times(self._h), "cfd_reset_kernel_times")
+
+    def reset_counters(self) -> None:
+        check(lib().cfd_reset_counters(self._h), "cfd_reset_counters")
+
+    def synchronize(self) -> None:
+        check(lib().cfd_synchronize(self._h), "cfd_synchronize")
+
+    def state_device(self):
+        p = C.c_void_p()
+        plane = C.c_int64()
+        pitch = C.c_int()
+        check(lib().cfd_state_device(self._h, C.byref(p), C.byref(plane), C.byref(pitch)),
+              "cfd_state_device")
+        return p.value, plane.value, pitch.value
+
+    def run_reference_loop(self, max_steps: int, n: int = 0, t: float = 0.0):
+        """The reference time loop (headers/simulation.hpp:48-61) driven from
+        the host: dt = compute_dt(n, t); step(dt); t += dt; n++; snap."""
+        T = self.cfg.T
+        taken = 0
+        while t < T and taken < max_steps:
+            dt = self.compute_dt(n, t)
+            self.step(dt)
+            t += dt
+            n += 1
+            taken += 1
+            if math.fabs(t - T) < 1e-12:
+                t = T
+        return taken, n, t

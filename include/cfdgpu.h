@@ -1,0 +1,170 @@
+/* cfdgpu.h -- C ABI of the B200 (sm_100a) split finite-volume solver for the
+ * 2D Euler equations and the Allaire five-equation two-material model.
+ *
+ * This is the drop-in boundary for cfd-art's time-stepping loop.  A caller
+ * that today drives the reference through its plugin interface
+ *   problem_base          euler_equations/euler_simulation_code/headers/problem_base.hpp:18-40
+ *   splitting_scheme_base euler_equations/euler_simulation_code/headers/splitting_scheme.hpp:22-27
+ *   simulation            euler_equations/euler_simulation_code/headers/simulation.hpp:36-67
+ * binds the functions below instead (see each declaration for the reference
+ * member it replaces).  Plain C types only; every function returns CFD_OK or a
+ * negative error code, and cfd_last_error() gives the message.
+ *
+ * Grids exchanged with the host use the reference's own layout unless stated
+ * otherwise: CFD_LAYOUT_GHOSTED_AOS is gridtype (headers/typedefs.hpp:19-21)
+ * flattened row-major, (ny + 2g) rows x (nx + 2g) cells x nvar doubles, with
+ * g = 2 ghost layers for MUSCL-Hancock and 1 for Godunov
+ * (sourcecode/euler_io.cpp:448-461), nvar = 4 (rho, rho u, rho v, E) for
+ * Euler and 6 (z rho1, (1-z) rho2, rho u, rho v, E, z) for Allaire.
+ */
+#ifndef CFDGPU_H
+#define CFDGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CFD_OK 0
+#define CFD_ERR_INVALID (-1)     /* bad argument or configuration */
+#define CFD_ERR_CUDA (-2)        /* CUDA runtime error (no device, launch failure, ...) */
+#define CFD_ERR_NOMEM (-3)       /* device or host allocation failed */
+#define CFD_ERR_STATE (-4)       /* call out of order (e.g. step before upload) */
+#define CFD_ERR_UNSUPPORTED (-5) /* option not available in this build */
+#define CFD_ERR_BUDGET (-6)      /* request exceeds the device-memory budget */
+
+enum { CFD_MODEL_EULER = 0, CFD_MODEL_ALLAIRE = 1 };
+enum { CFD_PREC_FP64 = 0, CFD_PREC_MIXED = 1 };
+enum { CFD_BC_TRANSMISSIVE = 0, CFD_BC_REFLECTIVE = 1 };
+enum { CFD_LIM_MINMOD = 0, CFD_LIM_VANLEER = 1, CFD_LIM_MC = 2, CFD_LIM_UNLIMITED = 3 };
+enum { CFD_FLUX_MUSCL = 0, CFD_FLUX_GODUNOV = 1 };
+enum { CFD_SPLIT_NAIVE = 0, CFD_SPLIT_STRANG = 1 };
+enum { CFD_WS_DAVIS = 0, CFD_WS_PVRS = 1 };
+enum { CFD_LAYOUT_GHOSTED_AOS = 0, CFD_LAYOUT_SOA = 1 };
+enum { CFD_BC_LEFT = 0, CFD_BC_RIGHT = 1, CFD_BC_BOTTOM = 2, CFD_BC_TOP = 3 };
+
+/* Event counters (cfd_status.counters); the reference prints or asserts. */
+enum {
+    CFD_CNT_UNPHYSICAL_INPUT = 0,  /* stencil state failing flux_solver_MUSCLhancock.hpp:131-134 */
+    CFD_CNT_SLOPE_ZEROED = 1,      /* flux_solver_MUSCLhancock.hpp:184-189 */
+    CFD_CNT_FIRST_ORDER = 2,       /* flux_solver_MUSCLhancock.hpp:216-223 */
+    CFD_CNT_FIXUP = 3,             /* sourcecode/euler_rowsweep.cpp:49-81 */
+    CFD_CNT_UNPHYSICAL_OUTPUT = 4  /* sourcecode/allaire_diffuse_rowsweep.cpp:49 */
+};
+
+/* Problem description.  Replaces the fields of sim_info
+ * (headers/sim_info.hpp:16-36) plus the EOS parameters (SGparams /
+ * binarySGparams, headers/stiffened_gas_eos.hpp:20-63) and the solver choices
+ * read from settingsfile.txt (headers/settings_file.hpp:19-72). */
+typedef struct cfd_config {
+    int model;            /* CFD_MODEL_* */
+    int precision;        /* CFD_PREC_* */
+    int nx, ny;           /* interior cells along x (columns) and y (rows), >= 2 */
+    double x0, y0, dx, dy;
+    double gamma1, pinf1; /* material 1 (Euler: the gas) */
+    double gamma2, pinf2; /* material 2 (Allaire) */
+    int bc[4];            /* CFD_BC_* per CFD_BC_LEFT..TOP */
+    double cfl;           /* CFL number (clamped to 0.2 for the first 5 steps) */
+    double T;             /* end time; the time loop stops at t >= T */
+    int limiter;          /* CFD_LIM_*; the reference uses minmod */
+    int flux_solver;      /* CFD_FLUX_* */
+    int splitting;        /* CFD_SPLIT_* */
+    int wavespeed;        /* CFD_WS_* (Allaire HLLC wave-speed estimate) */
+    double z_min;         /* Allaire: clip z to [z_min, 1 - z_min]; 0 = the reference's [0, 1] */
+    int fix_dy_halfstep;  /* 1: y-sweep half step uses dy (reference: dx, euler_colsweep.cpp:43) */
+    void* stream;         /* cudaStream_t to run on; NULL: the solver creates its own */
+} cfd_config;
+
+/* Snapshot of the device-resident time-loop state. */
+typedef struct cfd_status {
+    int n;                /* steps taken */
+    int done;             /* t >= T */
+    double t;             /* simulated time */
+    double dt_next;       /* dt compute_dt would return now (device rule) */
+    double maxu, maxv;    /* max(|u|+c), max(|v|+c) of the current state */
+    double mass1, mass2;  /* sum of rho*dx*dy (Allaire: of each partial density) */
+    unsigned long long counters[8];
+} cfd_status;
+
+typedef struct cfd_solver cfd_solver;
+
+/* Library identification (build string). */
+const char* cfd_version(void);
+
+/* Message of the last failing call on this thread; returns its length. */
+int cfd_last_error(char* buf, size_t len);
+
+/* Number of stored components per cell for a model (4 or 6). */
+int cfd_nvar(int model);
+
+/* Bytes of device memory cfd_create would allocate for cfg. */
+int cfd_device_bytes(const cfd_config* cfg, size_t* bytes);
+
+/* Allocates a solver and its device state.  Replaces problem->set_ICs'
+ * storage allocation (sourcecode/euler_io.cpp:494) and the construction of
+ * the flux/Riemann solver objects (:466-491). */
+int cfd_create(const cfd_config* cfg, cfd_solver** out);
+int cfd_destroy(cfd_solver* s);
+
+/* Copies an initial condition to the device and computes the wave speeds of
+ * it.  `host` is read in `layout`; ghost cells are ignored (they are rebuilt
+ * by every sweep, as pre_sweep does).  n and t set the step count and time. */
+int cfd_upload(cfd_solver* s, const double* host, int layout, int n, double t);
+
+/* Same from device memory (SoA planes of nx*ny doubles each, nvar planes). */
+int cfd_upload_device(cfd_solver* s, const double* dev_soa, int n, double t);
+
+/* Copies the current state to the host in `layout`.  In the ghosted layout
+ * the ghost strips hold the boundary fill of the current state. */
+int cfd_download(cfd_solver* s, double* host, int layout);
+
+/* problem_base::compute_dt (sourcecode/euler_timestep.cpp:7-44): dt for step
+ * n at time t from the current state.  Synchronises the solver's stream. */
+int cfd_compute_dt(cfd_solver* s, int n, double t, double* dt_out);
+
+/* splitting_scheme_base::advance_timestep (headers/splitting_scheme.hpp:26):
+ * one split step with the given dt (asynchronous on the solver's stream). */
+int cfd_step(cfd_solver* s, double dt);
+
+/* The time loop of headers/simulation.hpp:48-61 run on the device: up to
+ * max_steps steps with dt chosen on the device after each step, stopping at
+ * t >= T.  Asynchronous; steps past the end are no-ops. */
+int cfd_advance(cfd_solver* s, int max_steps);
+
+/* Waits for the solver's stream and returns the time-loop state. */
+int cfd_get_status(cfd_solver* s, cfd_status* st);
+
+/* Kernel timing for profiling: while enabled, every sweep launch is
+ * bracketed by CUDA events on the solver's stream (steps launch one by one
+ * instead of from the captured graph).  cfd_kernel_times returns the summed
+ * durations (ms) and launch counts per sweep direction (0: x, 1: y) since
+ * the last reset; it synchronises the stream. */
+int cfd_set_kernel_timing(cfd_solver* s, int enable);
+int cfd_kernel_times(cfd_solver* s, double ms[2], int launches[2]);
+int cfd_reset_kernel_times(cfd_solver* s);
+
+/* Resets the event counters. */
+int cfd_reset_counters(cfd_solver* s);
+
+/* Waits for all work queued on the solver's stream. */
+int cfd_synchronize(cfd_solver* s);
+
+/* Device-side layout of the current state for zero-copy callers: SoA planes
+ * `plane` elements apart, rows `pitch` elements apart, FP64. */
+int cfd_state_device(cfd_solver* s, const void** dev_ptr, int64_t* plane, int* pitch);
+
+/* ---- test entry: the device flux of single faces -------------------------
+ * flux_computation of the MUSCL-Hancock (or Godunov) solver
+ * (headers/flux_solver_MUSCLhancock.hpp:128-227 / A: :272-376) evaluated on
+ * the GPU for `nfaces` independent 4-cell (2-cell for Godunov) stencils of
+ * conserved states, host arrays.  flux: nfaces*nvar, u_star and z_star:
+ * nfaces each (z_star may be NULL for Euler). */
+int cfd_face_flux(const cfd_config* cfg, int nfaces, const double* stencils, double dt,
+                  double dx, double* flux, double* u_star, double* z_star);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

