@@ -49,6 +49,7 @@ SEED = 20261203
 WORKLOADS = {
     # name: (recipe, nx, ny, nbubbles)
     "euler4096": ("shock_bubbles", 4096, 4096, 32),
+    "euler2048": ("shock_bubbles", 2048, 2048, 32),  # smaller case for ncu captures
 }
 
 
@@ -212,6 +213,34 @@ def run_reference(args) -> None:
     }))
 
 
+def end_to_end(G, torch, cfg, ic, K, W, barrier, max_over_ranks, world, cells) -> dict:
+    """Same metric through the C ABI with host buffers: upload from pinned
+    memory, the reference-shaped host loop (compute_dt -> step), download."""
+    pinned_ic = torch.empty(ic.size, dtype=torch.float64, pin_memory=True)
+    pinned_ic.numpy()[:] = ic.ravel()
+    ic_pinned = pinned_ic.numpy().reshape(ic.shape)
+    pinned_out = torch.empty(ic.size, dtype=torch.float64, pin_memory=True)
+    out_pinned = pinned_out.numpy().reshape(ic.shape)
+    s2 = G.Solver(cfg)
+    s2.upload(ic_pinned)
+    s2.run_reference_loop(W)
+    s2.download(out=out_pinned)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s2.upload(ic_pinned)
+    taken, n2, t2 = s2.run_reference_loop(K)
+    s2.download(out=out_pinned)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    s2.close()
+    state_bytes = ic.size * 8
+    status_bytes = 96  # DevState read by compute_dt
+    return {"value": world * cells * taken / e2e_s / 1e9, "unit": UNIT,
+            "h2d_bytes_per_step": state_bytes / K,
+            "d2h_bytes_per_step": status_bytes + state_bytes / K, "seconds": e2e_s}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -220,6 +249,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="euler4096", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -299,29 +329,11 @@ def main() -> None:
     traffic = _profile_traffic(f"euler_{kname}")
 
     # ---- end to end through the C ABI with host buffers ------------------
-    pinned_ic = torch.empty(ic.size, dtype=torch.float64, pin_memory=True)
-    pinned_ic.numpy()[:] = ic.ravel()
-    ic_pinned = pinned_ic.numpy().reshape(ic.shape)
-    pinned_out = torch.empty(ic.size, dtype=torch.float64, pin_memory=True)
-    out_pinned = pinned_out.numpy().reshape(ic.shape)
-    s2 = G.Solver(cfg)
-    s2.upload(ic_pinned)
-    s2.run_reference_loop(W)
-    s2.download(out=out_pinned)
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    s2.upload(ic_pinned)
-    taken, n2, t2 = s2.run_reference_loop(K)
-    s2.download(out=out_pinned)
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = world * cells * taken / e2e_s / 1e9
-    s2.close()
+    e2e = None
+    if not args.no_e2e:
+        e2e = end_to_end(G, torch, cfg, ic, K, W, barrier, max_over_ranks, world, cells)
     s.close()
-    state_bytes = ic.size * 8
-    status_bytes = 96  # DevState read by compute_dt
-
+    
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(recipe, nbub)
@@ -343,10 +355,7 @@ def main() -> None:
                          "traffic": traffic,
                          "algorithmic_bytes_per_launch": bytes_launch,
                          "mean_launch_ms": [kms[0] / max(kn[0], 1), kms[1] / max(kn[1], 1)]},
-            "e2e": {"value": e2e_value, "unit": UNIT,
-                    "h2d_bytes_per_step": state_bytes / K,
-                    "d2h_bytes_per_step": status_bytes + state_bytes / K,
-                    "seconds": e2e_s},
+            "e2e": e2e,
             "cpu_baseline": cpu,
             "sim": {"n": st.n, "t": st.t, "counters": st.counter_dict()},
         }

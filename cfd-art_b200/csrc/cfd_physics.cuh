@@ -317,6 +317,25 @@ __device__ __forceinline__ void rp_side(const Eos& q, const double* U, RPSide<MO
     }
 }
 
+// flux_conserved_var (E/headers/misc_euler.hpp:20-39, A/headers/misc.hpp:31-52)
+// from the u and p the Riemann solver already derived from the same state.
+template <int MODEL>
+__device__ __forceinline__ void physical_flux(const double* U, const RPSide<MODEL>& S, double* F) {
+    if constexpr (MODEL == MODEL_EULER) {
+        F[0] = U[0] * S.u;
+        F[1] = (U[1] * S.u) + S.p;
+        F[2] = U[2] * S.u;
+        F[3] = (U[3] + S.p) * S.u;
+    } else {
+        F[0] = U[0] * S.u;
+        F[1] = U[1] * S.u;
+        F[2] = (U[2] * S.u) + S.p;
+        F[3] = U[3] * S.u;
+        F[4] = (U[4] + S.p) * S.u;
+        F[5] = 0.0;
+    }
+}
+
 // HLLC flux (E/headers/riemann_solver_HLLC.hpp:50-145,
 // A/headers/riemann_solver_HLLC.hpp:49-150).  The reference blends both star
 // fluxes with weights (1 +/- copysign(1,u*))/2, i.e. exactly 1 and 0; only
@@ -349,6 +368,41 @@ __device__ __forceinline__ void hllc_flux(const Eos& q, int wavespeed, const dou
                 ((L.rho * dSL) - (R.rho * dSR));
     u_star = us;
     bool left = !signbit(us);  // copysign(1.0, u*) == +1
+    // The unselected side enters the reference's blend multiplied by exactly
+    // 0, which only matters when it is not finite (0 * inf = NaN).  Its star
+    // factor dS / (S - u*) and p / dS are the only terms that can blow up
+    // from finite states; when either denominator is tiny the full blend is
+    // evaluated as the reference does.
+    double dS_o = left ? dSR : dSL;
+    double den_o = (left ? SR : SL) - us;
+    bool risky = !(fabs(dS_o) > 1e-200) || !(fabs(den_o) > 1e-200 * fabs(dS_o));
+    if (risky) {
+        double fL = dSL / (SL - us), fR = dSR / (SR - us);
+        double sL[NV], sR[NV], FL[NV], FR[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            sL[k] = fL * UL[k];
+            sR[k] = fR * UR[k];
+        }
+        sL[T::IM] = (fL * L.rho) * us;
+        sR[T::IM] = (fR * R.rho) * us;
+        sL[T::IE] = fL * (UL[T::IE] + ((us - L.u) * ((L.rho * us) + (L.p / dSL))));
+        sR[T::IE] = fR * (UR[T::IE] + ((us - R.u) * ((R.rho * us) + (R.p / dSR))));
+        physical_flux<MODEL>(UL, L, FL);
+        physical_flux<MODEL>(UR, R, FR);
+        if constexpr (MODEL == MODEL_ALLAIRE) {
+            sL[5] = 0.0;
+            sR[5] = 0.0;
+        }
+        double cs = copysign(1.0, us);
+        double a = (1.0 + cs) / 2.0, b = (1.0 - cs) / 2.0;
+        double mSL = smin(0.0, SL), MSR = smax(0.0, SR);
+#pragma unroll
+        for (int k = 0; k < NV; ++k)
+            F[k] = (a * (FL[k] + (mSL * (sL[k] - UL[k])))) + (b * (FR[k] + (MSR * (sR[k] - UR[k]))));
+        if constexpr (MODEL == MODEL_ALLAIRE) F[5] = 0.0;
+        return;
+    }
     const double* U = left ? UL : UR;
     const RPSide<MODEL>& S = left ? L : R;
     double Sk = left ? SL : SR;
@@ -360,22 +414,9 @@ __device__ __forceinline__ void hllc_flux(const Eos& q, int wavespeed, const dou
     for (int k = 0; k < NV; ++k) Us[k] = fac * U[k];
     Us[T::IM] = (fac * S.rho) * us;
     Us[T::IE] = fac * (U[T::IE] + ((us - S.u) * ((S.rho * us) + (S.p / dS))));
-    // physical flux of the selected side (flux_conserved_var, same u, p)
+    if constexpr (MODEL == MODEL_ALLAIRE) Us[5] = 0.0;
     double Fp[NV];
-    if constexpr (MODEL == MODEL_EULER) {
-        Fp[0] = U[0] * S.u;
-        Fp[1] = (U[1] * S.u) + S.p;
-        Fp[2] = U[2] * S.u;
-        Fp[3] = (U[3] + S.p) * S.u;
-    } else {
-        Fp[0] = U[0] * S.u;
-        Fp[1] = U[1] * S.u;
-        Fp[2] = (U[2] * S.u) + S.p;
-        Fp[3] = U[3] * S.u;
-        Fp[4] = (U[4] + S.p) * S.u;
-        Fp[5] = 0.0;
-        Us[5] = 0.0;
-    }
+    physical_flux<MODEL>(U, S, Fp);
 #pragma unroll
     for (int k = 0; k < NV; ++k) F[k] = Fp[k] + (wave * (Us[k] - U[k]));
     if constexpr (MODEL == MODEL_ALLAIRE) F[5] = 0.0;

@@ -224,7 +224,8 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
     const int cur = st->cur;
     const double* __restrict__ gin = A.bufs[cur ^ A.in_sel];
     double* __restrict__ gout = A.bufs[cur ^ A.in_sel ^ 1];
-    const double dt = A.dt_scale * (A.use_host_dt ? A.dt_host : st->dt);
+    const double dt_step = A.use_host_dt ? A.dt_host : st->dt;  // dt of the whole step
+    const double dt = A.dt_scale * dt_step;                        // this sweep's dt
     const Eos q = A.eos;
     const int len = (DIR == DIR_X) ? A.nx : A.ny;   // cells along the sweep
     const int wid = (DIR == DIR_X) ? A.ny : A.nx;   // lines
@@ -521,7 +522,7 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
     __syncthreads();
     if (is_last) {
         __threadfence();
-        finish_reduction(A.st, A.partials, gridDim.x, A.advance_time, dt, A.flip_cur);
+        finish_reduction(A.st, A.partials, gridDim.x, A.advance_time, dt_step, A.flip_cur);
     }
 }
 

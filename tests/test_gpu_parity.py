@@ -4,6 +4,8 @@ Bar: bit-identical FP64 results (np.array_equal, i.e. equal values; only
 the sign of an exact zero may differ), which implies the required relative
 L1 density error <= 1e-12 after the stated step count.
 """
+import zlib
+
 import numpy as np
 import pytest
 
@@ -62,7 +64,7 @@ def _random_stencils(model, n, rng, harsh):
 @pytest.mark.parametrize("limiter", ["minmod", "vanleer", "mc", "unlimited"])
 @pytest.mark.parametrize("harsh", [False, True])
 def test_device_faces_match_oracle(model, limiter, harsh):
-    rng = np.random.default_rng(hash((model, limiter, harsh)) % 2**32)
+    rng = np.random.default_rng(zlib.crc32(f"{model}-{limiter}-{harsh}".encode()))
     n = 4000
     st = _random_stencils(model, n, rng, harsh)
     if model == "euler":
@@ -78,7 +80,7 @@ def test_device_faces_match_oracle(model, limiter, harsh):
         rf, ru, rz = O.port_face_flux(model, p, st[f], dt, dx)
         ok = np.array_equal(flux[f], rf) or (np.isnan(rf).any() and np.array_equal(
             np.isnan(flux[f]), np.isnan(rf)))
-        assert ok, (f, flux[f], rf)
+        assert ok, (f, st[f].tolist(), flux[f].tolist(), rf.tolist())
         assert us[f] == ru or (np.isnan(ru) and np.isnan(us[f]))
         if model == "allaire" and not np.isnan(rz):
             assert zs[f] == rz
