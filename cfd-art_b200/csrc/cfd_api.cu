@@ -42,7 +42,7 @@ int fail(int code, const char* fmt, ...) {
 
 // Tile shapes: x-sweep 64 cells along x by 4 rows; y-sweep 32 cells along y
 // by 8 columns.
-constexpr int TSX = 64, NAX = 4, TSY = 32, NAY = 8;
+constexpr int TSX = 60, NAX = 4, TSY = 28, NAY = 8;
 
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
 

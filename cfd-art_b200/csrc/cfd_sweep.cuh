@@ -204,7 +204,7 @@ __host__ __device__ constexpr int sweep_smem_bytes() {
 }
 
 template <int MODEL, int DIR, int TS, int NA>
-__global__ void __launch_bounds__(256, 2) sweep_kernel(SweepArgs A) {
+__global__ void __launch_bounds__(256, MODEL == MODEL_EULER ? 3 : 2) sweep_kernel(SweepArgs A) {
     using Tl = SweepTile<MODEL, DIR, TS, NA>;
     using MT = ModelTraits<MODEL>;
     constexpr int NV = MT::NV;
