@@ -30,6 +30,7 @@ INC = [f"-I{ROOT / 'include'}", f"-I{PKG / 'csrc'}"]
 # (source, extra flags)
 CUDA_SOURCES = [
     ("csrc/cfd_api.cu", ["--fmad=false"]),
+    ("csrc/cfd_noalloc.cu", ["--fmad=false"]),
 ]
 HOST_SOURCES = ["host/ic.cpp", "host/io.cpp"]
 DRIVER = "host/driver.cpp"
@@ -43,7 +44,8 @@ def _newer(target: Path, deps: list[Path]) -> bool:
 
 
 def _headers() -> list[Path]:
-    return sorted((PKG / "csrc").glob("*.cuh")) + sorted((ROOT / "include").glob("*.h"))
+    return (sorted((PKG / "csrc").glob("*.cuh")) + sorted((PKG / "csrc").glob("*.h")) +
+            sorted((ROOT / "include").glob("*.h")))
 
 
 def _run(cmd: list[str], verbose: bool) -> None:

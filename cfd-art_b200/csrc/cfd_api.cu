@@ -14,15 +14,17 @@
 #include <vector>
 
 #include "../../include/cfdgpu.h"
+#include "cfd_error.h"
 #include "cfd_sweep.cuh"
 
 using namespace cfd;
 
 namespace {
-
 thread_local std::string g_err;
+}
 
-int fail(int code, const char* fmt, ...) {
+// Records the message cfd_last_error() returns on this thread.
+int cfd_fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -31,6 +33,10 @@ int fail(int code, const char* fmt, ...) {
     g_err = buf;
     return code;
 }
+
+namespace {
+
+#define fail cfd_fail
 
 #define CUDA_TRY(expr)                                                                   \
     do {                                                                                 \

@@ -92,7 +92,7 @@ __device__ __forceinline__ double choose_dt(const DevState& s, double maxu, doub
 
 // Last-CTA finish of the wave-speed reduction.  Partials are combined in CTA
 // order, so the mass sums are reproducible run to run.
-__device__ void finish_reduction(DevState* st, const double* partials, int nblocks,
+__device__ inline void finish_reduction(DevState* st, const double* partials, int nblocks,
                                  int advance_time, double dt_used, int flip_cur) {
     __shared__ double red[4][32];
     double mu = 0.0, mv = 0.0, m1 = 0.0, m2 = 0.0;

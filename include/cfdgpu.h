@@ -155,6 +155,30 @@ int cfd_synchronize(cfd_solver* s);
  * `plane` elements apart, rows `pitch` elements apart, FP64. */
 int cfd_state_device(cfd_solver* s, const void** dev_ptr, int64_t* plane, int* pitch);
 
+/* compute_dt without any device allocation, for callers that may not call
+ * cudaMalloc (inside someone else's CUDA graph capture, in a real-time loop
+ * with fixed memory, or in a host application that owns all device memory
+ * through its own pool).  No counterpart in the reference: it is the
+ * reference's compute_dt (sourcecode/euler_timestep.cpp:7-44) computed on a
+ * state the caller already holds on the device.
+ *   dev_state: SoA FP64 planes (nvar planes `plane` elements apart, rows
+ *              `pitch` elements apart), e.g. from cfd_state_device.
+ *   dev_out:   5 device doubles the caller owns, receiving dt (for step n at
+ *              time t, cfg's CFL and T), max(|u|+c), max(|v|+c) and the two
+ *              mass sums times dx*dy.
+ * The per-row reduction scratch is a fixed array inside the library,
+ * cfd_noalloc_max_rows() rows (8192) deep and 256 KiB in size, which every GPU
+ * that loads the library holds until exit; grids with more rows are rejected
+ * with CFD_ERR_INVALID.  Every call shares that array and it keeps the last
+ * call's contents, so calls that overlap on the GPU (concurrent streams or
+ * threads) race: serialise them.  The first call on each device looks up the
+ * array's device address with that device current; make that first call
+ * before any stream capture.  Asynchronous on `stream` (NULL: the legacy
+ * default stream); allocates nothing and frees nothing. */
+int cfd_compute_dt_noalloc(const cfd_config* cfg, const double* dev_state, int64_t plane,
+                           int pitch, int n, double t, double* dev_out, void* stream);
+int cfd_noalloc_max_rows(void);
+
 /* ---- test entry: the device flux of single faces -------------------------
  * flux_computation of the MUSCL-Hancock (or Godunov) solver
  * (headers/flux_solver_MUSCLhancock.hpp:128-227 / A: :272-376) evaluated on
