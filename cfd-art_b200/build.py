@@ -31,6 +31,8 @@ INC = [f"-I{ROOT / 'include'}", f"-I{PKG / 'csrc'}"]
 CUDA_SOURCES = [
     ("csrc/cfd_api.cu", ["--fmad=false"]),
     ("csrc/cfd_noalloc.cu", ["--fmad=false"]),
+    # mixed precision: FP32 with contraction and flush-to-zero
+    ("csrc/cfd_batch.cu", ["-ftz=true"]),
 ]
 HOST_SOURCES = ["host/ic.cpp", "host/io.cpp"]
 DRIVER = "host/driver.cpp"

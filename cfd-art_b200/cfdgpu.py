@@ -118,6 +118,22 @@ def lib() -> C.CDLL:
             "cfd_write_state": (ip, [cfgp, dp, C.c_char_p, C.c_double]),
             "cfd_write_schlieren": (ip, [cfgp, dp, C.c_char_p, C.c_double]),
             "cfd_write_masschange": (ip, [cfgp, C.c_char_p, ip, dp, dp, dp]),
+            "cfd_batch_create": (ip, [vp, C.c_size_t, C.POINTER(vp)]),
+            "cfd_batch_destroy": (ip, [vp]),
+            "cfd_batch_member_bytes": (ip, [cfgp, C.POINTER(C.c_size_t)]),
+            "cfd_batch_add": (ip, [vp, cfgp, dp, ip, C.POINTER(ip)]),
+            "cfd_batch_remove": (ip, [vp, ip]),
+            "cfd_batch_size": (ip, [vp, C.POINTER(ip), C.POINTER(C.c_size_t),
+                                    C.POINTER(C.c_size_t)]),
+            "cfd_batch_step": (ip, [vp, ip]),
+            "cfd_batch_step_timed": (ip, [vp, ip, dp, dp, C.POINTER(ip)]),
+            "cfd_batch_autotune": (ip, [vp, ip, dp]),
+            "cfd_batch_set_shapes": (ip, [vp, ip, ip, ip]),
+            "cfd_batch_get_shapes": (ip, [vp, ip, C.POINTER(ip), C.POINTER(ip)]),
+            "cfd_batch_status": (ip, [vp, ip, C.POINTER(Status)]),
+            "cfd_batch_poll": (ip, [vp, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip), dp,
+                                    C.POINTER(ip)]),
+            "cfd_batch_download": (ip, [vp, ip, dp, ip]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -280,3 +296,112 @@ class Solver:
             if math.fabs(t - T) < 1e-12:
                 t = T
         return taken, n, t
+
+
+class Batch:
+    """Batched mixed-precision solves (cfd_batch_*): members of uneven sizes
+    advanced together, each with its own dt and stop condition."""
+
+    def __init__(self, stream: int | None = None, budget_bytes: int = 0):
+        h = C.c_void_p()
+        check(lib().cfd_batch_create(C.c_void_p(stream) if stream else None, budget_bytes,
+                                     C.byref(h)), "cfd_batch_create")
+        self._h = h
+        self.cfgs: dict[int, Config] = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().cfd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @staticmethod
+    def member_bytes(cfg: Config) -> int:
+        n = C.c_size_t()
+        check(lib().cfd_batch_member_bytes(C.byref(cfg), C.byref(n)), "cfd_batch_member_bytes")
+        return n.value
+
+    def add(self, cfg: Config, grid: np.ndarray, max_steps: int = 0) -> int:
+        i = C.c_int()
+        check(lib().cfd_batch_add(self._h, C.byref(cfg), _dp(grid), max_steps, C.byref(i)),
+              "cfd_batch_add")
+        self.cfgs[i.value] = cfg.copy()
+        return i.value
+
+    def try_add(self, cfg: Config, grid: np.ndarray, max_steps: int = 0) -> int | None:
+        """Like add, but returns None when the member does not fit the budget."""
+        i = C.c_int()
+        rc = lib().cfd_batch_add(self._h, C.byref(cfg), _dp(grid), max_steps, C.byref(i))
+        if rc == -6:
+            return None
+        check(rc, "cfd_batch_add")
+        self.cfgs[i.value] = cfg.copy()
+        return i.value
+
+    def remove(self, mid: int) -> None:
+        check(lib().cfd_batch_remove(self._h, mid), "cfd_batch_remove")
+        self.cfgs.pop(mid, None)
+
+    def size(self):
+        n = C.c_int()
+        used = C.c_size_t()
+        budget = C.c_size_t()
+        check(lib().cfd_batch_size(self._h, C.byref(n), C.byref(used), C.byref(budget)),
+              "cfd_batch_size")
+        return n.value, used.value, budget.value
+
+    def step(self, ticks: int) -> None:
+        check(lib().cfd_batch_step(self._h, ticks), "cfd_batch_step")
+
+    def step_timed(self, ticks: int):
+        mx, my, n = C.c_double(), C.c_double(), C.c_int()
+        check(lib().cfd_batch_step_timed(self._h, ticks, C.byref(mx), C.byref(my), C.byref(n)),
+              "cfd_batch_step_timed")
+        return mx.value, my.value, n.value
+
+    def autotune(self, steps_per_trial: int = 2) -> float:
+        ms = C.c_double()
+        check(lib().cfd_batch_autotune(self._h, steps_per_trial, C.byref(ms)), "cfd_batch_autotune")
+        return ms.value
+
+    def set_shapes(self, model: int, sx: int, sy: int) -> None:
+        check(lib().cfd_batch_set_shapes(self._h, model, sx, sy), "cfd_batch_set_shapes")
+
+    def get_shapes(self, model: int):
+        a, b = C.c_int(), C.c_int()
+        check(lib().cfd_batch_get_shapes(self._h, model, C.byref(a), C.byref(b)),
+              "cfd_batch_get_shapes")
+        return a.value, b.value
+
+    def status(self, mid: int) -> Status:
+        st = Status()
+        check(lib().cfd_batch_status(self._h, mid, C.byref(st)), "cfd_batch_status")
+        return st
+
+    def poll(self):
+        n = len(self.cfgs) + 1
+        ids = (C.c_int * n)()
+        steps = (C.c_int * n)()
+        done = (C.c_int * n)()
+        t = (C.c_double * n)()
+        cnt = C.c_int()
+        check(lib().cfd_batch_poll(self._h, n, ids, steps, done, t, C.byref(cnt)), "cfd_batch_poll")
+        return [(ids[i], steps[i], bool(done[i]), t[i]) for i in range(cnt.value)]
+
+    def download(self, mid: int, layout: int = GHOSTED_AOS) -> np.ndarray:
+        c = self.cfgs[mid]
+        shape = c.ghosted_shape() if layout == GHOSTED_AOS else (c.nvar, c.ny, c.nx)
+        out = np.empty(shape)
+        check(lib().cfd_batch_download(self._h, mid, _dp(out), layout), "cfd_batch_download")
+        return out

@@ -1,0 +1,769 @@
+// Batched solves: many independent grids of uneven sizes advanced together.
+//
+// A batch owns device state for each member solve (instance) and advances
+// all active instances by one split step per "tick": one persistent x-sweep
+// launch and one persistent y-sweep launch per model present, over a tile
+// list that covers every active instance (csrc/cfd_mixed.cuh).  Each instance
+// keeps its own time-loop state (n, t, dt, T, max_steps), picks its own dt
+// after each step and stops on its own.  Ticks are captured into a CUDA graph
+// that is replayed until the membership changes.  Instances are admitted
+// against a device-memory budget, so a server can keep adding work while
+// others run.
+//
+// Precision: the mixed form (FP32 + compensation word state; see
+// cfd_mixed.cuh).  The plain FP64 form uses cfd_solver (cfd_api.cu).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/cfdgpu.h"
+#include "cfd_error.h"
+#include "cfd_mixed.cuh"
+
+using namespace cfd;
+using namespace cfd::mixed;
+
+namespace {
+
+#define BTRY(expr)                                                                          \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return cfd_fail(e_ == cudaErrorMemoryAllocation ? CFD_ERR_NOMEM : CFD_ERR_CUDA, \
+                            "%s: %s", #expr, cudaGetErrorString(e_));                       \
+    } while (0)
+
+// Tile-shape variants the autotuner chooses from: (TS along, NA across),
+// each keeping every phase of a 256-thread CTA a single pass.
+struct Shape {
+    int ts, na;
+};
+constexpr Shape kShapesX[] = {{60, 4}, {124, 2}, {28, 8}};
+constexpr Shape kShapesY[] = {{28, 8}, {60, 4}, {12, 16}};
+constexpr int kNumShapes = 3;
+
+template <int MODEL, int DIR, int TS, int NA>
+int launch_t(const MixedArgs& a, int grid, cudaStream_t st) {
+    constexpr int smem = MTile<MODEL, DIR, TS, NA>::SMEM;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(mixed_sweep_kernel<MODEL, DIR, TS, NA>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "smem attribute: %s", cudaGetErrorString(e));
+        attr = true;
+    }
+    mixed_sweep_kernel<MODEL, DIR, TS, NA><<<grid, 256, smem, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "mixed sweep launch: %s", cudaGetErrorString(e));
+    return CFD_OK;
+}
+
+template <int MODEL>
+int launch_shape(int dir, int shape, const MixedArgs& a, int grid, cudaStream_t st) {
+    if (dir == DIR_X) {
+        switch (shape) {
+            case 0: return launch_t<MODEL, DIR_X, 60, 4>(a, grid, st);
+            case 1: return launch_t<MODEL, DIR_X, 124, 2>(a, grid, st);
+            default: return launch_t<MODEL, DIR_X, 28, 8>(a, grid, st);
+        }
+    }
+    switch (shape) {
+        case 0: return launch_t<MODEL, DIR_Y, 28, 8>(a, grid, st);
+        case 1: return launch_t<MODEL, DIR_Y, 60, 4>(a, grid, st);
+        default: return launch_t<MODEL, DIR_Y, 12, 16>(a, grid, st);
+    }
+}
+
+int tiles_for(int nx, int ny, int dir, Shape s) {
+    int len = dir == DIR_X ? nx : ny, wid = dir == DIR_X ? ny : nx;
+    return ((len + s.ts - 1) / s.ts) * ((wid + s.na - 1) / s.na);
+}
+
+// ---- conversion kernels ----------------------------------------------------
+
+__global__ void ghosted_to_mixed(const double* __restrict__ src, float* __restrict__ hi,
+                                 float* __restrict__ lo, double* __restrict__ soa, int nx, int ny,
+                                 int g, int nv, int pitch, long long plane) {
+    long long n = (long long)nx * ny;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(idx / nx), j = (int)(idx % nx);
+        const double* c = src + ((long long)(i + g) * (nx + 2 * g) + (j + g)) * nv;
+        long long o = (long long)i * pitch + j;
+        for (int k = 0; k < nv; ++k) {
+            double x = c[k];
+            float h = (float)x;
+            hi[k * plane + o] = h;
+            lo[k * plane + o] = (float)(x - (double)h);
+            soa[k * plane + o] = x;
+        }
+    }
+}
+
+__global__ void mixed_to_ghosted(const float* __restrict__ hi, const float* __restrict__ lo,
+                                 double* __restrict__ dst, int nx, int ny, int g, int nv, int pitch,
+                                 long long plane, int bcL, int bcR, int bcB, int bcT, int im, int it) {
+    int W = nx + 2 * g, H = ny + 2 * g;
+    long long n = (long long)W * H;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int gi = (int)(idx / W), gj = (int)(idx % W);
+        int i = gi - g, j = gj - g;
+        double* d = dst + idx * nv;
+        bool ri = i >= 0 && i < ny, rj = j >= 0 && j < nx;
+        if (!ri && !rj) {
+            for (int k = 0; k < nv; ++k) d[k] = 0.0;
+            continue;
+        }
+        int si = i, sj = j, neg = -1;
+        if (j < 0) { sj = -j - 1; if (bcL) neg = im; }
+        else if (j >= nx) { sj = 2 * nx - 1 - j; if (bcR) neg = im; }
+        if (i < 0) { si = -i - 1; if (bcB) neg = it; }
+        else if (i >= ny) { si = 2 * ny - 1 - i; if (bcT) neg = it; }
+        long long o = (long long)si * pitch + sj;
+        for (int k = 0; k < nv; ++k) {
+            double v = (double)hi[k * plane + o] + (double)lo[k * plane + o];
+            d[k] = (k == neg) ? -v : v;
+        }
+    }
+}
+
+template <int MODEL>
+__global__ void init_reduce(const double* __restrict__ in, long long plane, int pitch, int nx,
+                            int ny, Eos q, DevState* st, double* partials) {
+    constexpr int NV = ModelTraits<MODEL>::NV;
+    double r_mu = 0.0, r_mv = 0.0, r_m1 = 0.0, r_m2 = 0.0;
+    long long n = (long long)nx * ny;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(idx / nx), j = (int)(idx % nx);
+        double U[NV];
+        for (int k = 0; k < NV; ++k) U[k] = in[k * plane + (long long)i * pitch + j];
+        double su, sv, m1, m2;
+        wave_speeds<MODEL>(q, U, su, sv, m1, m2);
+        r_mu = smax(r_mu, su);
+        r_mv = smax(r_mv, sv);
+        r_m1 += m1;
+        r_m2 += m2;
+    }
+    __shared__ double red[4][32];
+    __shared__ bool is_last;
+    for (int o = 16; o > 0; o >>= 1) {
+        r_mu = smax(r_mu, __shfl_down_sync(0xffffffffu, r_mu, o));
+        r_mv = smax(r_mv, __shfl_down_sync(0xffffffffu, r_mv, o));
+        r_m1 += __shfl_down_sync(0xffffffffu, r_m1, o);
+        r_m2 += __shfl_down_sync(0xffffffffu, r_m2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = r_mu;
+        red[1][threadIdx.x >> 5] = r_mv;
+        red[2][threadIdx.x >> 5] = r_m1;
+        red[3][threadIdx.x >> 5] = r_m2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mu = red[0][0], mv = red[1][0], m1 = red[2][0], m2 = red[3][0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            mu = smax(mu, red[0][w]);
+            mv = smax(mv, red[1][w]);
+            m1 += red[2][w];
+            m2 += red[3][w];
+        }
+        double* p = partials + 4 * blockIdx.x;
+        p[0] = mu;
+        p[1] = mv;
+        p[2] = m1;
+        p[3] = m2;
+        __threadfence();
+        is_last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        finish_reduction(st, partials, gridDim.x, 0, 0.0, 0);
+    }
+}
+
+constexpr int kInitBlocks = 148 * 2;
+
+struct Member {
+    int id;
+    cfd_config cfg;
+    Inst inst;          // host copy of the device descriptor
+    void* mem = nullptr;  // one allocation: buffers, state, partials
+    size_t bytes = 0;
+    int max_steps;
+};
+
+}  // namespace
+
+struct cfd_batch {
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    size_t budget = 0, used = 0;
+    int next_id = 1;
+    std::vector<Member> members;
+    Inst* d_insts = nullptr;
+    int d_insts_cap = 0;
+    // tile lists per (model, dir): device arrays
+    int* d_tiles = nullptr;
+    size_t d_tiles_cap = 0;
+    struct Group {
+        int model, dir, shape, ntiles, offset;
+    };
+    std::vector<Group> groups;
+    bool dirty = true;
+    int shape[2][2] = {{0, 0}, {0, 0}};  // [model][dir]
+    int sms = 148;
+    // graph of `graph_steps` ticks for the current membership
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    // autotuning state
+    bool tuned = false;
+    int tune_override = -1;
+};
+
+namespace {
+
+int build_tables(cfd_batch* b) {
+    if (!b->dirty) return CFD_OK;
+    std::vector<int> all;
+    b->groups.clear();
+    std::vector<Inst> insts(b->members.size());
+    for (size_t i = 0; i < b->members.size(); ++i) {
+        Member& m = b->members[i];
+        int model = m.cfg.model;
+        m.inst.tiles_x = tiles_for(m.cfg.nx, m.cfg.ny, DIR_X, kShapesX[b->shape[model][DIR_X]]);
+        m.inst.tiles_y = tiles_for(m.cfg.nx, m.cfg.ny, DIR_Y, kShapesY[b->shape[model][DIR_Y]]);
+        insts[i] = m.inst;
+    }
+    // largest instances first within each group so the tail of a sweep is
+    // made of small tiles of small solves
+    std::vector<int> order(b->members.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::sort(order.begin(), order.end(), [&](int x, int y) {
+        return (long long)b->members[x].cfg.nx * b->members[x].cfg.ny >
+               (long long)b->members[y].cfg.nx * b->members[y].cfg.ny;
+    });
+    for (int model = 0; model < 2; ++model)
+        for (int dir = 0; dir < 2; ++dir) {
+            cfd_batch::Group g;
+            g.model = model;
+            g.dir = dir;
+            g.shape = b->shape[model][dir];
+            g.offset = (int)all.size() / 2;
+            std::vector<int> ti, tl;
+            for (int idx : order) {
+                const Member& m = b->members[idx];
+                if (m.cfg.model != model) continue;
+                int nt = dir == DIR_X ? insts[idx].tiles_x : insts[idx].tiles_y;
+                for (int t = 0; t < nt; ++t) {
+                    ti.push_back(idx);
+                    tl.push_back(t);
+                }
+            }
+            g.ntiles = (int)ti.size();
+            if (!g.ntiles) continue;
+            // store as [inst..., local...] pairs: inst at offset, local at offset + ntiles
+            g.offset = (int)all.size();
+            all.insert(all.end(), ti.begin(), ti.end());
+            all.insert(all.end(), tl.begin(), tl.end());
+            b->groups.push_back(g);
+        }
+    if ((int)insts.size() > b->d_insts_cap) {
+        cudaFree(b->d_insts);
+        b->d_insts = nullptr;
+        int cap = std::max<int>(16, (int)insts.size() * 2);
+        BTRY(cudaMalloc(&b->d_insts, sizeof(Inst) * cap));
+        b->d_insts_cap = cap;
+    }
+    if (all.size() > b->d_tiles_cap) {
+        cudaFree(b->d_tiles);
+        b->d_tiles = nullptr;
+        size_t cap = std::max<size_t>(1024, all.size() * 2);
+        BTRY(cudaMalloc(&b->d_tiles, sizeof(int) * cap));
+        b->d_tiles_cap = cap;
+    }
+    if (!insts.empty())
+        BTRY(cudaMemcpyAsync(b->d_insts, insts.data(), sizeof(Inst) * insts.size(),
+                             cudaMemcpyHostToDevice, b->stream));
+    if (!all.empty())
+        BTRY(cudaMemcpyAsync(b->d_tiles, all.data(), sizeof(int) * all.size(),
+                             cudaMemcpyHostToDevice, b->stream));
+    BTRY(cudaStreamSynchronize(b->stream));  // host vectors die at return
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->dirty = false;
+    return CFD_OK;
+}
+
+int persistent_grid(const cfd_batch* b, int ntiles) {
+    // 2 CTAs per SM of 256 threads keep the FP32 sweeps fed; never more CTAs
+    // than tiles
+    return std::max(1, std::min(ntiles, b->sms * 2));
+}
+
+struct Timed {
+    int group;
+    cudaEvent_t e0, e1;
+};
+
+int enqueue_tick(cfd_batch* b, std::vector<Timed>* timing) {
+    for (int dir = 0; dir < 2; ++dir)
+        for (int gi = 0; gi < (int)b->groups.size(); ++gi) {
+            const auto& g = b->groups[gi];
+            if (g.dir != dir) continue;
+            MixedArgs a;
+            a.insts = b->d_insts;
+            a.tile_inst = b->d_tiles + g.offset;
+            a.tile_local = b->d_tiles + g.offset + g.ntiles;
+            a.ntiles = g.ntiles;
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            if (timing) {
+                cudaEventCreate(&e0);
+                cudaEventCreate(&e1);
+                cudaEventRecord(e0, b->stream);
+            }
+            int grid = persistent_grid(b, g.ntiles);
+            int r = g.model == CFD_MODEL_EULER
+                        ? launch_shape<MODEL_EULER>(dir, g.shape, a, grid, b->stream)
+                        : launch_shape<MODEL_ALLAIRE>(dir, g.shape, a, grid, b->stream);
+            if (timing) {
+                cudaEventRecord(e1, b->stream);
+                timing->push_back({gi, e0, e1});
+            }
+            if (r) return r;
+        }
+    return CFD_OK;
+}
+
+size_t member_bytes(const cfd_config& c, size_t* plane_out, int* pitch_out) {
+    int nv = cfd_nvar(c.model);
+    int pitch = (c.nx + 31) / 32 * 32;
+    size_t plane = (size_t)pitch * c.ny;
+    int ty = 0;
+    for (int s = 0; s < kNumShapes; ++s)
+        ty = std::max(ty, std::max(tiles_for(c.nx, c.ny, DIR_Y, kShapesY[s]),
+                                   tiles_for(c.nx, c.ny, DIR_X, kShapesX[s])));
+    int npart = std::max(ty, kInitBlocks);
+    size_t bytes = 4 * sizeof(float) * nv * plane  // hi/lo x 2 buffers
+                   + 256 + sizeof(DevState) + 4 * sizeof(double) * npart + 4096;
+    if (plane_out) *plane_out = plane;
+    if (pitch_out) *pitch_out = pitch;
+    return bytes;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfd_batch_create(void* stream, size_t device_budget_bytes, cfd_batch** out) {
+    if (!out) return cfd_fail(CFD_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return cfd_fail(CFD_ERR_CUDA, "no CUDA device available");
+    cfd_batch* b = new (std::nothrow) cfd_batch();
+    if (!b) return cfd_fail(CFD_ERR_NOMEM, "host allocation failed");
+    if (stream) {
+        b->stream = (cudaStream_t)stream;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete b;
+            return cfd_fail(CFD_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+        }
+        b->own_stream = true;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+    if (device_budget_bytes == 0) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        device_budget_bytes = (size_t)(0.8 * (double)fr);
+    }
+    b->budget = device_budget_bytes;
+    *out = b;
+    return CFD_OK;
+}
+
+int cfd_batch_destroy(cfd_batch* b) {
+    if (!b) return CFD_OK;
+    cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (auto& m : b->members) cudaFree(m.mem);
+    cudaFree(b->d_insts);
+    cudaFree(b->d_tiles);
+    if (b->own_stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return CFD_OK;
+}
+
+int cfd_batch_member_bytes(const cfd_config* cfg, size_t* bytes) {
+    if (!cfg || !bytes) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    *bytes = member_bytes(*cfg, nullptr, nullptr);
+    return CFD_OK;
+}
+
+int cfd_batch_add(cfd_batch* b, const cfd_config* cfg, const double* host_ic, int max_steps,
+                  int* id_out) {
+    if (!b || !cfg || !host_ic || !id_out) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    const cfd_config& c = *cfg;
+    if (c.model != CFD_MODEL_EULER && c.model != CFD_MODEL_ALLAIRE)
+        return cfd_fail(CFD_ERR_INVALID, "unknown model %d", c.model);
+    if (c.nx < 2 || c.ny < 2) return cfd_fail(CFD_ERR_INVALID, "grid %dx%d too small", c.nx, c.ny);
+    if (c.splitting != CFD_SPLIT_NAIVE)
+        return cfd_fail(CFD_ERR_UNSUPPORTED, "batched solves use naive splitting");
+    if (!(c.gamma1 > 1.0) || (c.model == CFD_MODEL_ALLAIRE && !(c.gamma2 > 1.0)))
+        return cfd_fail(CFD_ERR_INVALID, "gamma must be > 1");
+    if (max_steps <= 0) max_steps = 0x7fffffff;
+    size_t plane;
+    int pitch;
+    size_t bytes = member_bytes(c, &plane, &pitch);
+    if (b->used + bytes > b->budget)
+        return cfd_fail(CFD_ERR_BUDGET, "instance needs %zu bytes, %zu of %zu in use", bytes,
+                        b->used, b->budget);
+    Member m;
+    m.id = b->next_id++;
+    m.cfg = c;
+    m.max_steps = max_steps;
+    m.bytes = bytes;
+    BTRY(cudaMalloc(&m.mem, bytes));
+    int nv = cfd_nvar(c.model);
+    char* p = static_cast<char*>(m.mem);
+    auto take = [&](size_t n) {
+        char* q = p;
+        p += (n + 255) / 256 * 256;
+        return q;
+    };
+    Inst& I = m.inst;
+    memset(&I, 0, sizeof I);
+    for (int k = 0; k < 2; ++k) {
+        I.hi[k] = reinterpret_cast<float*>(take(sizeof(float) * nv * plane));
+        I.lo[k] = reinterpret_cast<float*>(take(sizeof(float) * nv * plane));
+    }
+    I.st = reinterpret_cast<DevState*>(take(sizeof(DevState)));
+    int npart = (int)((bytes - 4 * sizeof(float) * nv * plane - 256 - sizeof(DevState) - 4096) /
+                      (4 * sizeof(double)));
+    I.partials = reinterpret_cast<double*>(take(4 * sizeof(double) * npart));
+    I.plane = (long long)plane;
+    I.pitch = pitch;
+    I.nx = c.nx;
+    I.ny = c.ny;
+    I.nv = nv;
+    I.model = c.model;
+    I.limiter = c.limiter;
+    I.wavespeed = c.wavespeed;
+    I.godunov = c.flux_solver == CFD_FLUX_GODUNOV;
+    I.fix_dy = c.fix_dy_halfstep;
+    for (int k = 0; k < 4; ++k) I.bc[k] = c.bc[k];
+    I.dx = c.dx;
+    I.dy = c.dy;
+    I.z_min = c.z_min;
+    I.eos.g1 = c.gamma1;
+    I.eos.p1 = c.pinf1;
+    I.eos.g2 = c.model == CFD_MODEL_ALLAIRE ? c.gamma2 : 1.4;
+    I.eos.p2 = c.model == CFD_MODEL_ALLAIRE ? c.pinf2 : 0.0;
+    I.eos.gm1_1 = I.eos.g1 - 1.0;
+    I.eos.gm1_2 = I.eos.g2 - 1.0;
+    I.eos.gp1 = I.eos.g1 * I.eos.p1;
+    I.g1f = (float)I.eos.g1;
+    I.p1f = (float)I.eos.p1;
+    I.g2f = (float)I.eos.g2;
+    I.p2f = (float)I.eos.p2;
+    I.gm1_1f = (float)I.eos.gm1_1;
+    I.gm1_2f = (float)I.eos.gm1_2;
+    I.gp1f = (float)I.eos.gp1;
+    I.max_steps = max_steps;
+    I.active = 1;
+    // upload: the ghosted FP64 grid goes through the second buffer pair as
+    // staging (its 2 x nv x plane floats hold the ghosted doubles when the
+    // grid is large enough; otherwise a temporary buffer is used)
+    int g = c.flux_solver == CFD_FLUX_GODUNOV ? 1 : 2;
+    size_t ghosted = (size_t)nv * (c.nx + 2 * g) * (size_t)(c.ny + 2 * g);
+    size_t soa = (size_t)nv * plane;
+    double* staging = nullptr;
+    cudaError_t e = cudaMalloc(&staging, sizeof(double) * (ghosted + soa));
+    if (e != cudaSuccess) {
+        cudaFree(m.mem);
+        return cfd_fail(CFD_ERR_NOMEM, "staging: %s", cudaGetErrorString(e));
+    }
+    DevState init;
+    memset(&init, 0, sizeof init);
+    init.T = c.T;
+    init.cfl = c.cfl;
+    init.dx = c.dx;
+    init.dy = c.dy;
+    int r = CFD_OK;
+    do {
+        if ((e = cudaMemcpyAsync(I.st, &init, sizeof init, cudaMemcpyHostToDevice, b->stream)) ||
+            (e = cudaMemcpyAsync(staging, host_ic, sizeof(double) * ghosted, cudaMemcpyHostToDevice,
+                                 b->stream))) {
+            r = cfd_fail(CFD_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+            break;
+        }
+        ghosted_to_mixed<<<148 * 4, 256, 0, b->stream>>>(staging, I.hi[0], I.lo[0],
+                                                         staging + ghosted, c.nx, c.ny, g, nv,
+                                                         pitch, (long long)plane);
+        if (c.model == CFD_MODEL_EULER)
+            init_reduce<MODEL_EULER><<<kInitBlocks, 256, 0, b->stream>>>(
+                staging + ghosted, (long long)plane, pitch, c.nx, c.ny, I.eos, I.st, I.partials);
+        else
+            init_reduce<MODEL_ALLAIRE><<<kInitBlocks, 256, 0, b->stream>>>(
+                staging + ghosted, (long long)plane, pitch, c.nx, c.ny, I.eos, I.st, I.partials);
+        if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(b->stream))) {
+            r = cfd_fail(CFD_ERR_CUDA, "upload kernels: %s", cudaGetErrorString(e));
+            break;
+        }
+    } while (0);
+    cudaFree(staging);
+    if (r) {
+        cudaFree(m.mem);
+        return r;
+    }
+    b->used += bytes;
+    b->members.push_back(m);
+    b->dirty = true;
+    *id_out = m.id;
+    return CFD_OK;
+}
+
+static Member* find(cfd_batch* b, int id) {
+    for (auto& m : b->members)
+        if (m.id == id) return &m;
+    return nullptr;
+}
+
+int cfd_batch_remove(cfd_batch* b, int id) {
+    if (!b) return cfd_fail(CFD_ERR_INVALID, "null batch");
+    for (size_t i = 0; i < b->members.size(); ++i)
+        if (b->members[i].id == id) {
+            BTRY(cudaStreamSynchronize(b->stream));
+            cudaFree(b->members[i].mem);
+            b->used -= b->members[i].bytes;
+            b->members.erase(b->members.begin() + i);
+            b->dirty = true;
+            return CFD_OK;
+        }
+    return cfd_fail(CFD_ERR_INVALID, "no instance %d", id);
+}
+
+int cfd_batch_size(cfd_batch* b, int* count, size_t* used, size_t* budget) {
+    if (!b) return cfd_fail(CFD_ERR_INVALID, "null batch");
+    if (count) *count = (int)b->members.size();
+    if (used) *used = b->used;
+    if (budget) *budget = b->budget;
+    return CFD_OK;
+}
+
+int cfd_batch_set_shapes(cfd_batch* b, int model, int shape_x, int shape_y) {
+    if (!b || model < 0 || model > 1 || shape_x < 0 || shape_x >= kNumShapes || shape_y < 0 ||
+        shape_y >= kNumShapes)
+        return cfd_fail(CFD_ERR_INVALID, "bad shape selection");
+    b->shape[model][DIR_X] = shape_x;
+    b->shape[model][DIR_Y] = shape_y;
+    b->dirty = true;
+    b->tuned = true;
+    return CFD_OK;
+}
+
+int cfd_batch_get_shapes(cfd_batch* b, int model, int* shape_x, int* shape_y) {
+    if (!b || model < 0 || model > 1) return cfd_fail(CFD_ERR_INVALID, "bad arguments");
+    if (shape_x) *shape_x = b->shape[model][DIR_X];
+    if (shape_y) *shape_y = b->shape[model][DIR_Y];
+    return CFD_OK;
+}
+
+// Autotuner: runs `steps_per_trial` real steps with each tile shape per model
+// and sweep direction, keeps the fastest per cell (CUDA events).  The results
+// of the mixed sweeps do not depend on the tiling, so the trial steps are
+// ordinary steps of the solves.
+int cfd_batch_autotune(cfd_batch* b, int steps_per_trial, double* best_ms) {
+    if (!b) return cfd_fail(CFD_ERR_INVALID, "null batch");
+    if (steps_per_trial < 1) steps_per_trial = 1;
+    double best_tick = 0.0;
+    for (int model = 0; model < 2; ++model) {
+        bool present = false;
+        for (auto& m : b->members) present |= m.cfg.model == model;
+        if (!present) continue;
+        for (int dir = 0; dir < 2; ++dir) {
+            double best = 1e300;
+            int best_s = b->shape[model][dir];
+            for (int s = 0; s < kNumShapes; ++s) {
+                b->shape[model][dir] = s;
+                b->dirty = true;
+                int r = build_tables(b);
+                if (r) return r;
+                std::vector<Timed> ev;
+                for (int k = 0; k < steps_per_trial; ++k)
+                    if ((r = enqueue_tick(b, &ev))) return r;
+                BTRY(cudaStreamSynchronize(b->stream));
+                double ms = 0.0;
+                for (auto& t : ev) {
+                    const auto& g = b->groups[t.group];
+                    if (g.model == model && g.dir == dir) {
+                        float m = 0.f;
+                        cudaEventElapsedTime(&m, t.e0, t.e1);
+                        ms += m;
+                    }
+                    cudaEventDestroy(t.e0);
+                    cudaEventDestroy(t.e1);
+                }
+                ms /= steps_per_trial;
+                if (ms < best) {
+                    best = ms;
+                    best_s = s;
+                }
+            }
+            b->shape[model][dir] = best_s;
+            b->dirty = true;
+            best_tick += best;
+        }
+    }
+    b->tuned = true;
+    if (best_ms) *best_ms = best_tick;
+    return build_tables(b);
+}
+
+int cfd_batch_step(cfd_batch* b, int ticks) {
+    if (!b) return cfd_fail(CFD_ERR_INVALID, "null batch");
+    if (ticks <= 0 || b->members.empty()) return CFD_OK;
+    int r = build_tables(b);
+    if (r) return r;
+    const int K = 8;
+    if (ticks >= K) {
+        if (!b->graph) {
+            BTRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            int rr = CFD_OK;
+            for (int i = 0; i < K && rr == CFD_OK; ++i) rr = enqueue_tick(b, nullptr);
+            cudaGraph_t gph;
+            cudaError_t e = cudaStreamEndCapture(b->stream, &gph);
+            if (rr) return rr;
+            if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "capture: %s", cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&b->graph, gph, 0);
+            cudaGraphDestroy(gph);
+            if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
+            b->graph_steps = K;
+        }
+        for (int i = 0; i + K <= ticks; i += K) BTRY(cudaGraphLaunch(b->graph, b->stream));
+    }
+    for (int i = 0; i < ticks % K; ++i)
+        if ((r = enqueue_tick(b, nullptr))) return r;
+    return CFD_OK;
+}
+
+int cfd_batch_step_timed(cfd_batch* b, int ticks, double* ms_x, double* ms_y, int* launches) {
+    if (!b) return cfd_fail(CFD_ERR_INVALID, "null batch");
+    int r = build_tables(b);
+    if (r) return r;
+    std::vector<Timed> ev;
+    for (int i = 0; i < ticks; ++i)
+        if ((r = enqueue_tick(b, &ev))) return r;
+    BTRY(cudaStreamSynchronize(b->stream));
+    double sx = 0, sy = 0;
+    for (auto& t : ev) {
+        float m = 0.f;
+        cudaEventElapsedTime(&m, t.e0, t.e1);
+        if (b->groups[t.group].dir == DIR_X) sx += m;
+        else sy += m;
+        cudaEventDestroy(t.e0);
+        cudaEventDestroy(t.e1);
+    }
+    if (ms_x) *ms_x = sx;
+    if (ms_y) *ms_y = sy;
+    if (launches) *launches = (int)ev.size();
+    return CFD_OK;
+}
+
+int cfd_batch_status(cfd_batch* b, int id, cfd_status* out) {
+    if (!b || !out) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    Member* m = find(b, id);
+    if (!m) return cfd_fail(CFD_ERR_INVALID, "no instance %d", id);
+    DevState d;
+    BTRY(cudaMemcpyAsync(&d, m->inst.st, sizeof d, cudaMemcpyDeviceToHost, b->stream));
+    BTRY(cudaStreamSynchronize(b->stream));
+    memset(out, 0, sizeof *out);
+    out->n = d.n;
+    out->done = d.done || d.n >= m->max_steps;
+    out->t = d.t;
+    out->dt_next = d.dt;
+    out->maxu = d.maxu;
+    out->maxv = d.maxv;
+    out->mass1 = d.mass1;
+    out->mass2 = d.mass2;
+    return CFD_OK;
+}
+
+// Status of every member in one device-to-host copy: ids, steps taken and a
+// done flag per member (arrays of `cap` entries); returns the count.
+int cfd_batch_poll(cfd_batch* b, int cap, int* ids, int* steps, int* done, double* t, int* count) {
+    if (!b || !count) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    int n = (int)b->members.size();
+    *count = n;
+    std::vector<DevState> ds(n);
+    for (int i = 0; i < n; ++i)
+        BTRY(cudaMemcpyAsync(&ds[i], b->members[i].inst.st, sizeof(DevState),
+                             cudaMemcpyDeviceToHost, b->stream));
+    BTRY(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < n && i < cap; ++i) {
+        if (ids) ids[i] = b->members[i].id;
+        if (steps) steps[i] = ds[i].n;
+        if (done) done[i] = ds[i].done || ds[i].n >= b->members[i].max_steps;
+        if (t) t[i] = ds[i].t;
+    }
+    return CFD_OK;
+}
+
+int cfd_batch_download(cfd_batch* b, int id, double* host, int layout) {
+    if (!b || !host) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    Member* m = find(b, id);
+    if (!m) return cfd_fail(CFD_ERR_INVALID, "no instance %d", id);
+    const cfd_config& c = m->cfg;
+    DevState d;
+    BTRY(cudaMemcpyAsync(&d, m->inst.st, sizeof d, cudaMemcpyDeviceToHost, b->stream));
+    BTRY(cudaStreamSynchronize(b->stream));
+    int cur = d.cur & 1;
+    int nv = cfd_nvar(c.model), g = c.flux_solver == CFD_FLUX_GODUNOV ? 1 : 2;
+    size_t elems = layout == CFD_LAYOUT_GHOSTED_AOS
+                       ? (size_t)nv * (c.nx + 2 * g) * (size_t)(c.ny + 2 * g)
+                       : (size_t)nv * c.nx * c.ny;
+    double* tmp = nullptr;
+    BTRY(cudaMalloc(&tmp, sizeof(double) * elems));
+    int im = c.model == CFD_MODEL_EULER ? 1 : 2;
+    if (layout == CFD_LAYOUT_GHOSTED_AOS) {
+        mixed_to_ghosted<<<148 * 4, 256, 0, b->stream>>>(
+            m->inst.hi[cur], m->inst.lo[cur], tmp, c.nx, c.ny, g, nv, m->inst.pitch,
+            m->inst.plane, c.bc[0], c.bc[1], c.bc[2], c.bc[3], im, im + 1);
+    } else {
+        // SoA interior: reuse the ghosted kernel with g = 0 and no boundary
+        mixed_to_ghosted<<<148 * 4, 256, 0, b->stream>>>(m->inst.hi[cur], m->inst.lo[cur], tmp,
+                                                         c.nx, c.ny, 0, nv, m->inst.pitch,
+                                                         m->inst.plane, 0, 0, 0, 0, -1, -1);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(host, tmp, sizeof(double) * elems, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "download: %s", cudaGetErrorString(e));
+    if (layout == CFD_LAYOUT_SOA) {
+        // the kernel wrote AoS interior; reorder to SoA planes on the host
+        std::vector<double> aos(host, host + elems);
+        size_t cells = (size_t)c.nx * c.ny;
+        for (size_t q = 0; q < cells; ++q)
+            for (int k = 0; k < nv; ++k) host[k * cells + q] = aos[q * nv + k];
+    }
+    return CFD_OK;
+}
+
+}  // extern "C"

@@ -179,6 +179,43 @@ int cfd_compute_dt_noalloc(const cfd_config* cfg, const double* dev_state, int64
                            int pitch, int n, double t, double* dev_out, void* stream);
 int cfd_noalloc_max_rows(void);
 
+/* ---- batched solves (mixed precision) -------------------------------------
+ * Many independent solves of uneven sizes advanced together: each tick runs
+ * one persistent x-sweep launch and one y-sweep launch per model over the
+ * tiles of every active member, every member choosing its own dt and
+ * stopping on its own (at t >= T or after max_steps).  Members use the mixed
+ * form: FP32 reconstruction and Riemann solves, state stored as FP32 plus an
+ * FP32 compensation word, FP64 for stiffened-gas pressure recovery, the CFL
+ * reduction and time.  No counterpart in the reference, which runs one
+ * problem per process (euler_equations/euler_simulation_code/sourcecode/main.cpp:17-49).
+ * Members are admitted against a device-memory budget (bytes; 0 = 80 % of the
+ * free memory at creation); cfd_batch_add returns CFD_ERR_BUDGET when a
+ * member does not fit. */
+typedef struct cfd_batch cfd_batch;
+int cfd_batch_create(void* stream, size_t device_budget_bytes, cfd_batch** out);
+int cfd_batch_destroy(cfd_batch* b);
+/* Device bytes one member of cfg would take. */
+int cfd_batch_member_bytes(const cfd_config* cfg, size_t* bytes);
+/* Adds a solve from a ghosted AoS initial grid (cfg.splitting must be
+ * naive); max_steps <= 0 runs to T.  Synchronous; returns the member id. */
+int cfd_batch_add(cfd_batch* b, const cfd_config* cfg, const double* host_ic, int max_steps,
+                  int* id_out);
+int cfd_batch_remove(cfd_batch* b, int id);
+int cfd_batch_size(cfd_batch* b, int* count, size_t* used_bytes, size_t* budget_bytes);
+/* Advances every member by `ticks` steps (members that are done idle). */
+int cfd_batch_step(cfd_batch* b, int ticks);
+/* Same, one launch at a time with CUDA events: summed x- and y-sweep ms. */
+int cfd_batch_step_timed(cfd_batch* b, int ticks, double* ms_x, double* ms_y, int* launches);
+/* Autotuner: tries each tile shape per model and sweep direction on real
+ * steps (results do not depend on the tiling) and keeps the fastest. */
+int cfd_batch_autotune(cfd_batch* b, int steps_per_trial, double* best_tick_ms);
+int cfd_batch_set_shapes(cfd_batch* b, int model, int shape_x, int shape_y);
+int cfd_batch_get_shapes(cfd_batch* b, int model, int* shape_x, int* shape_y);
+int cfd_batch_status(cfd_batch* b, int id, cfd_status* st);
+/* ids, steps taken, done flags and times of all members (cap entries). */
+int cfd_batch_poll(cfd_batch* b, int cap, int* ids, int* steps, int* done, double* t, int* count);
+int cfd_batch_download(cfd_batch* b, int id, double* host, int layout);
+
 /* ---- test entry: the device flux of single faces -------------------------
  * flux_computation of the MUSCL-Hancock (or Godunov) solver
  * (headers/flux_solver_MUSCLhancock.hpp:128-227 / A: :272-376) evaluated on

@@ -1,0 +1,144 @@
+"""Mixed-precision batched form: accuracy against the FP64 path, batching
+invariance (a member's result does not depend on what else is in the batch or
+on the tile shapes), per-member stop conditions and budget admission."""
+import numpy as np
+import pytest
+
+import cfdgpu as G
+from cfdtest import density, load_golden, rel_l1
+
+pytestmark = pytest.mark.gpu
+TOL_MIXED_L1 = 1e-4  # relative L1 density error of the mixed form vs FP64
+
+
+def _fp64_run(cfg, ic, steps):
+    with G.Solver(cfg) as s:
+        s.upload(ic)
+        s.advance(steps)
+        st = s.status()
+        return s.download(), st
+
+
+def _mixed_run(cfg, ic, steps):
+    with G.Batch() as b:
+        i = b.add(cfg, ic, max_steps=steps)
+        b.step(steps)
+        st = b.status(i)
+        return b.download(i), st
+
+
+def _errors(a, b, model):
+    ra = density(a[2:-2, 2:-2], model)
+    rb = density(b[2:-2, 2:-2], model)
+    return rel_l1(ra, rb), float(np.abs(ra - rb).max() / np.abs(rb).max())
+
+
+def test_mixed_four_quadrant_vs_reference_golden():
+    fx = load_golden("euler_four_quadrant_200x200")
+    cfg = G.recipe_config("four_quadrant", 200, 200)
+    ic = G.recipe_ic(cfg, "four_quadrant")
+    out, st = _mixed_run(cfg, ic, 100000)
+    assert st.t == 0.3
+    l1 = rel_l1(out[2:-2, 2:-2, 0], fx["rho"])
+    linf = float(np.abs(out[2:-2, 2:-2, 0] - fx["rho"]).max() / fx["rho"].max())
+    print(f"four-quadrant 200^2 to t=0.3: mixed vs reference L1 {l1:.2e} Linf {linf:.2e}")
+    assert l1 <= TOL_MIXED_L1
+
+
+@pytest.mark.parametrize("recipe,nx,ny,steps", [
+    ("shock_bubbles", 512, 512, 300),
+    ("water_shock_air_bubble", 256, 128, 300),
+])
+def test_mixed_vs_fp64(recipe, nx, ny, steps):
+    cfg = G.recipe_config(recipe, nx, ny)
+    ic = G.recipe_ic(cfg, recipe, nbubbles=32)
+    ref, sr = _fp64_run(cfg, ic, steps)
+    out, sm = _mixed_run(cfg, ic, steps)
+    assert sm.n == sr.n == steps
+    assert abs(sm.t - sr.t) <= 1e-4 * sr.t
+    model = "euler" if cfg.model == G.EULER else "allaire"
+    l1, linf = _errors(out, ref, model)
+    print(f"{recipe} {nx}x{ny} {steps} steps: mixed vs FP64 L1 {l1:.2e} Linf {linf:.2e}")
+    assert np.isfinite(out).all()
+    assert l1 <= TOL_MIXED_L1
+
+
+@pytest.mark.parametrize("case,nx,ny", [("ST2_x", 200, 20), ("cross", 96, 80),
+                                        ("shocked_helium_bubble", 130, 36)])
+def test_mixed_reference_cases(case, nx, ny):
+    model = G.ALLAIRE if case in ("ST2_x", "shocked_helium_bubble") else G.EULER
+    cfg = G.case_config(model, case, nx, ny)
+    ic = G.case_ic(cfg, case)
+    steps = 150
+    ref, sr = _fp64_run(cfg, ic, steps)
+    out, sm = _mixed_run(cfg, ic, steps)
+    l1, linf = _errors(out, ref, "euler" if model == G.EULER else "allaire")
+    print(f"{case}: mixed vs FP64 L1 {l1:.2e} Linf {linf:.2e} (n={sm.n}, t={sm.t:.4g})")
+    assert l1 <= TOL_MIXED_L1
+
+
+def _members():
+    out = []
+    for k, (rec, nx, ny) in enumerate([("shock_bubbles", 96, 200), ("shock_bubbles", 300, 64),
+                                       ("water_shock_air_bubble", 128, 64),
+                                       ("shock_bubbles", 64, 64),
+                                       ("water_shock_air_bubble", 90, 45)]):
+        cfg = G.recipe_config(rec, nx, ny)
+        out.append((cfg, G.recipe_ic(cfg, rec, seed=100 + k, nbubbles=6), 40 + 5 * k))
+    return out
+
+
+def test_member_alone_equals_member_in_mix():
+    mem = _members()
+    with G.Batch() as b:
+        ids = [b.add(c, ic, steps) for c, ic, steps in mem]
+        b.step(80)  # more ticks than any member needs
+        mixed = [b.download(i) for i in ids]
+        stats = [b.status(i) for i in ids]
+    for (c, ic, steps), out, st in zip(mem, mixed, stats):
+        assert st.n == steps and st.done
+        alone, st1 = _mixed_run(c, ic, steps)
+        assert st1.n == st.n and st1.t == st.t
+        assert np.array_equal(alone, out)
+
+
+def test_tile_shapes_do_not_change_results():
+    mem = _members()[:3]
+    outs = []
+    for shape in range(3):
+        with G.Batch() as b:
+            for model in (G.EULER, G.ALLAIRE):
+                b.set_shapes(model, shape, shape)
+            ids = [b.add(c, ic, 20) for c, ic, _ in mem]
+            b.step(20)
+            outs.append([b.download(i) for i in ids])
+    for k in range(len(mem)):
+        assert np.array_equal(outs[0][k], outs[1][k]) and np.array_equal(outs[0][k], outs[2][k])
+
+
+def test_autotune_keeps_results_and_picks_shapes():
+    mem = _members()
+    with G.Batch() as b:
+        ids = [b.add(c, ic, 30) for c, ic, _ in mem]
+        ms = b.autotune(2)  # 2 x 3 shapes x 2 sweeps x 2 models steps of real work
+        assert ms > 0
+        b.step(30)
+        tuned = [b.download(i) for i in ids]
+    for (c, ic, _), out in zip(mem, tuned):
+        alone, _ = _mixed_run(c, ic, 30)
+        assert np.array_equal(alone, out)
+
+
+def test_budget_admission():
+    cfg = G.recipe_config("shock_bubbles", 512, 512)
+    ic = G.recipe_ic(cfg, "shock_bubbles", nbubbles=4)
+    need = G.Batch.member_bytes(cfg)
+    with G.Batch(budget_bytes=int(need * 2.5)) as b:
+        a1 = b.try_add(cfg, ic, 10)
+        a2 = b.try_add(cfg, ic, 10)
+        a3 = b.try_add(cfg, ic, 10)
+        assert a1 is not None and a2 is not None and a3 is None
+        n, used, budget = b.size()
+        assert n == 2 and used <= budget
+        b.remove(a1)
+        assert b.try_add(cfg, ic, 10) is not None
