@@ -32,9 +32,9 @@ CUDA_SOURCES = [
     ("csrc/cfd_api.cu", ["--fmad=false"]),
     ("csrc/cfd_noalloc.cu", ["--fmad=false"]),
     # mixed precision: FP32 with contraction and flush-to-zero
-    ("csrc/cfd_batch.cu", ["-ftz=true"]),
+    ("csrc/cfd_batch.cu", ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
 ]
-HOST_SOURCES = ["host/ic.cpp", "host/io.cpp"]
+HOST_SOURCES = ["host/ic.cpp", "host/io.cpp", "host/server.cpp"]
 DRIVER = "host/driver.cpp"
 
 
@@ -73,12 +73,13 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         s = PKG / src
         o = OBJ / (Path(src).stem + ".o")
         if force or not _newer(o, [s, *hdrs]):
-            _run([CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", *INC, "-c",
-                  str(s), "-o", str(o)], verbose)
+            _run([CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", *INC,
+                  "-I/usr/local/cuda/include", "-pthread", "-c", str(s), "-o", str(o)], verbose)
         objs.append(o)
     so = LIB / "libcfdgpu.so"
     if force or not _newer(so, objs):
-        _run([NVCC, *ARCH, "-shared", "-o", str(so), *map(str, objs)], verbose)
+        _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-pthread", "-o", str(so), *map(str, objs)],
+             verbose)
     drv = PKG / DRIVER
     exe = LIB / "run-cfd-simulation"
     if drv.exists() and (force or not _newer(exe, [drv, so, *hdrs])):

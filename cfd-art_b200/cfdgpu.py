@@ -77,6 +77,27 @@ class Status(C.Structure):
         return {k: int(self.counters[i]) for i, k in enumerate(COUNTERS)}
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("precision", C.c_int), ("budget_bytes", C.c_size_t),
+                ("budget_fraction", C.c_double), ("ticks_per_round", C.c_int),
+                ("stream", C.c_void_p)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("error", C.c_int), ("steps", C.c_int), ("t", C.c_double),
+                ("submit_s", C.c_double), ("queue_s", C.c_double), ("run_s", C.c_double),
+                ("latency_s", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_int64), ("admitted", C.c_int64), ("queued", C.c_int64),
+                ("running", C.c_int64), ("max_running", C.c_int64), ("rounds", C.c_int64),
+                ("cell_updates", C.c_double), ("busy_s", C.c_double), ("wall_s", C.c_double),
+                ("used_bytes", C.c_size_t), ("budget_bytes", C.c_size_t)]
+
+
+REQ_DONE, REQ_FAILED = 2, 3
+
 _lib: C.CDLL | None = None
 
 
@@ -134,6 +155,12 @@ def lib() -> C.CDLL:
             "cfd_batch_poll": (ip, [vp, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip), dp,
                                     C.POINTER(ip)]),
             "cfd_batch_download": (ip, [vp, ip, dp, ip]),
+            "cfd_server_create": (ip, [C.POINTER(ServerOptions), C.POINTER(vp)]),
+            "cfd_server_submit": (ip, [vp, cfgp, dp, ip, C.POINTER(C.c_int64)]),
+            "cfd_server_wait": (ip, [vp, C.c_int64, C.c_double, C.POINTER(RequestInfo), dp]),
+            "cfd_server_release": (ip, [vp, C.c_int64]),
+            "cfd_server_get_stats": (ip, [vp, C.POINTER(ServerStats)]),
+            "cfd_server_destroy": (ip, [vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -405,3 +432,57 @@ class Batch:
         out = np.empty(shape)
         check(lib().cfd_batch_download(self._h, mid, _dp(out), layout), "cfd_batch_download")
         return out
+
+
+class Server:
+    """Continuous-batching server (cfd_server_*): submit solves from any
+    thread, wait for their final grids; a worker thread owns the GPU."""
+
+    def __init__(self, precision: int = MIXED, budget_bytes: int = 0, budget_fraction: float = 0.8,
+                 ticks_per_round: int = 16, stream: int | None = None):
+        o = ServerOptions(precision, budget_bytes, budget_fraction, ticks_per_round,
+                          C.c_void_p(stream) if stream else None)
+        h = C.c_void_p()
+        check(lib().cfd_server_create(C.byref(o), C.byref(h)), "cfd_server_create")
+        self._h = h
+        self.cfgs: dict[int, Config] = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().cfd_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, cfg: Config, grid: np.ndarray, steps: int) -> int:
+        rid = C.c_int64()
+        check(lib().cfd_server_submit(self._h, C.byref(cfg), _dp(np.ascontiguousarray(grid)),
+                                      steps, C.byref(rid)), "cfd_server_submit")
+        self.cfgs[rid.value] = cfg.copy()
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = -1.0, want_result: bool = True):
+        info = RequestInfo()
+        out = np.empty(self.cfgs[rid].ghosted_shape()) if want_result else None
+        check(lib().cfd_server_wait(self._h, rid, timeout, C.byref(info),
+                                    _dp(out) if out is not None else None), "cfd_server_wait")
+        return info, out
+
+    def release(self, rid: int) -> None:
+        check(lib().cfd_server_release(self._h, rid), "cfd_server_release")
+        self.cfgs.pop(rid, None)
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        check(lib().cfd_server_get_stats(self._h, C.byref(st)), "cfd_server_get_stats")
+        return st

@@ -49,16 +49,21 @@ constexpr Shape kShapesX[] = {{60, 4}, {124, 2}, {28, 8}};
 constexpr Shape kShapesY[] = {{28, 8}, {60, 4}, {12, 16}};
 constexpr int kNumShapes = 3;
 
+// Persistent launch: as many CTAs as fit on the device at once (occupancy
+// of this variant), never more than there are tiles.
 template <int MODEL, int DIR, int TS, int NA>
-int launch_t(const MixedArgs& a, int grid, cudaStream_t st) {
+int launch_t(const MixedArgs& a, int sms, cudaStream_t st) {
     constexpr int smem = MTile<MODEL, DIR, TS, NA>::SMEM;
-    static bool attr = false;
-    if (!attr) {
+    static int per_sm = 0;
+    if (!per_sm) {
         cudaError_t e = cudaFuncSetAttribute(mixed_sweep_kernel<MODEL, DIR, TS, NA>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "smem attribute: %s", cudaGetErrorString(e));
-        attr = true;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, mixed_sweep_kernel<MODEL, DIR, TS, NA>, 256, smem);
+        if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     }
+    int grid = std::max(1, std::min(a.ntiles, per_sm * sms));
     mixed_sweep_kernel<MODEL, DIR, TS, NA><<<grid, 256, smem, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "mixed sweep launch: %s", cudaGetErrorString(e));
@@ -306,12 +311,6 @@ int build_tables(cfd_batch* b) {
     return CFD_OK;
 }
 
-int persistent_grid(const cfd_batch* b, int ntiles) {
-    // 2 CTAs per SM of 256 threads keep the FP32 sweeps fed; never more CTAs
-    // than tiles
-    return std::max(1, std::min(ntiles, b->sms * 2));
-}
-
 struct Timed {
     int group;
     cudaEvent_t e0, e1;
@@ -333,7 +332,7 @@ int enqueue_tick(cfd_batch* b, std::vector<Timed>* timing) {
                 cudaEventCreate(&e1);
                 cudaEventRecord(e0, b->stream);
             }
-            int grid = persistent_grid(b, g.ntiles);
+            int grid = b->sms;
             int r = g.model == CFD_MODEL_EULER
                         ? launch_shape<MODEL_EULER>(dir, g.shape, a, grid, b->stream)
                         : launch_shape<MODEL_ALLAIRE>(dir, g.shape, a, grid, b->stream);

@@ -51,9 +51,12 @@ struct MixedArgs {
     int ntiles;             // tiles of this launch; CTAs loop over them (persistent)
 };
 
-__device__ __forceinline__ float frcp(float x) { return __frcp_rn(x); }
-__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
-__device__ __forceinline__ float fsqrt(float x) { return __fsqrt_rn(x); }
+// This translation unit is compiled with -prec-div=false -prec-sqrt=false:
+// single-precision division, reciprocal and square root use the hardware
+// approximations (about 1-2 ulp), ample for the FP32 face arithmetic.
+__device__ __forceinline__ float frcp(float x) { return 1.0f / x; }
+__device__ __forceinline__ float fdiv(float a, float b) { return a / b; }
+__device__ __forceinline__ float fsqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ float fminf_s(float a, float b) { return (b < a) ? b : a; }
 __device__ __forceinline__ float fmaxf_s(float a, float b) { return (a < b) ? b : a; }
 

@@ -1,0 +1,343 @@
+// Continuous-batching server for split finite-volume solves.
+//
+// Clients submit solves (configuration, initial grid, step count) at any
+// time from any thread.  A worker thread owns the GPU: between rounds of
+// `ticks_per_round` batched steps it admits queued requests in arrival order
+// as device memory (the budget) frees up, keeps every admitted solve's state
+// resident on the device, advances all of them together, and returns each
+// finished solve's grid to its client, recording queue, run and completion
+// times.  Requests that arrive while others run join the next round, so
+// their work overlaps on the device with the work already there.
+//
+// Mixed precision serves through cfd_batch (one persistent launch per sweep
+// for all members); plain FP64 serves each member with its own cfd_solver on
+// the worker's stream.  No counterpart in the reference (one problem per
+// process, euler_equations/euler_simulation_code/sourcecode/main.cpp:17-49).
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/cfdgpu.h"
+#include "../../include/cfdgpu_host.h"
+#include "../csrc/cfd_error.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double secs(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double>(b - a).count();
+}
+
+struct Request {
+    int64_t id;
+    cfd_config cfg;
+    std::vector<double> ic;   // ghosted AoS initial grid; reused for the result
+    int steps;
+    int state = CFD_REQ_QUEUED;
+    int error = 0;
+    Clock::time_point t_submit, t_admit, t_done;
+    int member = -1;          // batch member id (mixed)
+    cfd_solver* solver = nullptr;  // FP64
+    int issued = 0;                // FP64: steps enqueued so far
+    size_t bytes = 0;
+    cfd_status final_status{};
+};
+
+}  // namespace
+
+struct cfd_server {
+    cfd_server_options opt{};
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<int64_t> queue;
+    std::map<int64_t, std::unique_ptr<Request>> reqs;
+    std::vector<int64_t> running;
+    int64_t next_id = 1;
+    bool stop = false;
+    std::thread worker;
+    cfd_batch* batch = nullptr;
+    cudaStream_t stream = nullptr;
+    size_t budget = 0, used = 0;
+    Clock::time_point t0;
+    // statistics
+    double cell_updates = 0.0;
+    double busy_s = 0.0;
+    int64_t completed = 0, rounds = 0, admitted = 0;
+    int max_running = 0;
+    int worker_error = 0;
+    int device = 0;
+};
+
+namespace {
+
+size_t fp64_bytes(const cfd_config& c) {
+    size_t b = 0;
+    cfd_device_bytes(&c, &b);
+    return b;
+}
+
+// Admission under the lock: FIFO, but a request that does not fit does not
+// block smaller ones behind it (it keeps its place at the head).
+void admit(cfd_server* s, std::vector<Request*>& to_start) {
+    size_t free_b = s->budget > s->used ? s->budget - s->used : 0;
+    for (auto it = s->queue.begin(); it != s->queue.end();) {
+        Request* r = s->reqs[*it].get();
+        size_t need = 0;
+        if (s->opt.precision == CFD_PREC_MIXED) cfd_batch_member_bytes(&r->cfg, &need);
+        else need = fp64_bytes(r->cfg);
+        if (need <= free_b) {
+            free_b -= need;
+            s->used += need;
+            r->bytes = need;
+            r->state = CFD_REQ_RUNNING;
+            r->t_admit = Clock::now();
+            to_start.push_back(r);
+            it = s->queue.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
+void finish(cfd_server* s, Request* r, int err) {
+    r->t_done = Clock::now();
+    r->error = err;
+    r->state = err ? CFD_REQ_FAILED : CFD_REQ_DONE;
+    s->used -= r->bytes;
+    if (!err) {
+        s->completed++;
+        s->cell_updates += (double)r->cfg.nx * r->cfg.ny * r->final_status.n;
+    }
+}
+
+void worker_main(cfd_server* s) {
+    cudaSetDevice(s->device);
+    const int K = std::max(1, s->opt.ticks_per_round);
+    while (true) {
+        std::vector<Request*> start;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty() || !s->running.empty(); });
+            if (s->stop) break;
+            admit(s, start);
+        }
+        // start admitted requests (device allocation + upload)
+        for (Request* r : start) {
+            int rc;
+            if (s->opt.precision == CFD_PREC_MIXED) {
+                rc = cfd_batch_add(s->batch, &r->cfg, r->ic.data(), r->steps, &r->member);
+            } else {
+                cfd_config c = r->cfg;
+                c.stream = s->stream;
+                c.T = r->cfg.T;
+                rc = cfd_create(&c, &r->solver);
+                if (!rc) rc = cfd_upload(r->solver, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS, 0, 0.0);
+            }
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (rc) {
+                finish(s, r, rc);
+                s->cv_done.notify_all();
+            } else {
+                s->running.push_back(r->id);
+                s->admitted++;
+            }
+        }
+        std::vector<Request*> run;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            for (int64_t id : s->running) run.push_back(s->reqs[id].get());
+            s->max_running = std::max<int>(s->max_running, (int)run.size());
+        }
+        if (run.empty()) continue;
+        auto tr = Clock::now();
+        // one round of batched steps
+        if (s->opt.precision == CFD_PREC_MIXED) {
+            if (cfd_batch_step(s->batch, K)) s->worker_error = CFD_ERR_CUDA;
+        } else {
+            for (Request* r : run) {
+                int k = std::min(K, r->steps - r->issued);
+                if (k > 0 && cfd_advance(r->solver, k) == CFD_OK) r->issued += k;
+            }
+        }
+        // completion check: one status read per member
+        std::vector<Request*> done;
+        for (Request* r : run) {
+            cfd_status st;
+            int rc = s->opt.precision == CFD_PREC_MIXED ? cfd_batch_status(s->batch, r->member, &st)
+                                                         : cfd_get_status(r->solver, &st);
+            if (rc || st.done || st.n >= r->steps) {
+                r->final_status = st;
+                done.push_back(r);
+            }
+        }
+        for (Request* r : done) {
+            int rc;
+            if (s->opt.precision == CFD_PREC_MIXED) {
+                rc = cfd_batch_download(s->batch, r->member, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS);
+                cfd_batch_remove(s->batch, r->member);
+            } else {
+                rc = cfd_download(r->solver, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS);
+                cfd_destroy(r->solver);
+                r->solver = nullptr;
+            }
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->running.erase(std::find(s->running.begin(), s->running.end(), r->id));
+            finish(s, r, rc);
+        }
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->busy_s += secs(tr, Clock::now());
+            s->rounds++;
+        }
+        if (!done.empty()) s->cv_done.notify_all();
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfd_server_create(const cfd_server_options* opt, cfd_server** out) {
+    if (!opt || !out) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    if (opt->precision != CFD_PREC_MIXED && opt->precision != CFD_PREC_FP64)
+        return cfd_fail(CFD_ERR_INVALID, "bad precision");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return cfd_fail(CFD_ERR_CUDA, "no CUDA device available");
+    auto* s = new cfd_server();
+    s->opt = *opt;
+    if (s->opt.ticks_per_round <= 0) s->opt.ticks_per_round = 16;
+    cudaGetDevice(&s->device);
+    s->stream = (cudaStream_t)opt->stream;
+    if (!s->stream) cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    s->budget = opt->budget_bytes ? opt->budget_bytes
+                                  : (size_t)((opt->budget_fraction > 0 ? opt->budget_fraction : 0.8) *
+                                             (double)fr);
+    if (opt->precision == CFD_PREC_MIXED) {
+        int rc = cfd_batch_create(s->stream, (size_t)-1 / 2, &s->batch);
+        if (rc) {
+            delete s;
+            return rc;
+        }
+    }
+    s->t0 = Clock::now();
+    s->worker = std::thread(worker_main, s);
+    *out = s;
+    return CFD_OK;
+}
+
+int cfd_server_submit(cfd_server* s, const cfd_config* cfg, const double* ic, int steps,
+                      int64_t* id_out) {
+    if (!s || !cfg || !ic || !id_out || steps <= 0) return cfd_fail(CFD_ERR_INVALID, "bad argument");
+    size_t elems = 0;
+    cfd_ic_grid_elems(cfg, &elems);
+    auto r = std::make_unique<Request>();
+    r->cfg = *cfg;
+    r->cfg.stream = nullptr;
+    r->ic.assign(ic, ic + elems);
+    r->steps = steps;
+    r->t_submit = Clock::now();
+    size_t need = 0;
+    if (s->opt.precision == CFD_PREC_MIXED) cfd_batch_member_bytes(cfg, &need);
+    else need = fp64_bytes(*cfg);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (need > s->budget)
+        return cfd_fail(CFD_ERR_BUDGET, "request needs %zu bytes, the budget is %zu", need, s->budget);
+    r->id = s->next_id++;
+    *id_out = r->id;
+    s->queue.push_back(r->id);
+    s->reqs[r->id] = std::move(r);
+    s->cv_work.notify_one();
+    return CFD_OK;
+}
+
+int cfd_server_wait(cfd_server* s, int64_t id, double timeout_s, cfd_request_info* info,
+                    double* result) {
+    if (!s) return cfd_fail(CFD_ERR_INVALID, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return cfd_fail(CFD_ERR_INVALID, "no request %lld", (long long)id);
+    Request* r = it->second.get();
+    auto pred = [&] { return r->state == CFD_REQ_DONE || r->state == CFD_REQ_FAILED; };
+    if (timeout_s < 0) s->cv_done.wait(lk, pred);
+    else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred)) {
+        if (info) {
+            memset(info, 0, sizeof *info);
+            info->state = r->state;
+        }
+        return CFD_OK;
+    }
+    if (info) {
+        memset(info, 0, sizeof *info);
+        info->state = r->state;
+        info->error = r->error;
+        info->steps = r->final_status.n;
+        info->t = r->final_status.t;
+        info->queue_s = secs(r->t_submit, r->t_admit);
+        info->run_s = secs(r->t_admit, r->t_done);
+        info->latency_s = secs(r->t_submit, r->t_done);
+        info->submit_s = secs(s->t0, r->t_submit);
+    }
+    if (result && r->state == CFD_REQ_DONE) memcpy(result, r->ic.data(), r->ic.size() * sizeof(double));
+    return r->state == CFD_REQ_FAILED ? cfd_fail(r->error, "request %lld failed", (long long)id)
+                                      : CFD_OK;
+}
+
+int cfd_server_release(cfd_server* s, int64_t id) {
+    if (!s) return cfd_fail(CFD_ERR_INVALID, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return cfd_fail(CFD_ERR_INVALID, "no request");
+    if (it->second->state != CFD_REQ_DONE && it->second->state != CFD_REQ_FAILED)
+        return cfd_fail(CFD_ERR_STATE, "request still in flight");
+    s->reqs.erase(it);
+    return CFD_OK;
+}
+
+int cfd_server_get_stats(cfd_server* s, cfd_server_stats* st) {
+    if (!s || !st) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    memset(st, 0, sizeof *st);
+    st->completed = s->completed;
+    st->admitted = s->admitted;
+    st->queued = (int64_t)s->queue.size();
+    st->running = (int64_t)s->running.size();
+    st->max_running = s->max_running;
+    st->rounds = s->rounds;
+    st->cell_updates = s->cell_updates;
+    st->busy_s = s->busy_s;
+    st->wall_s = secs(s->t0, Clock::now());
+    st->used_bytes = s->used;
+    st->budget_bytes = s->budget;
+    return CFD_OK;
+}
+
+int cfd_server_destroy(cfd_server* s) {
+    if (!s) return CFD_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    for (auto& kv : s->reqs)
+        if (kv.second->solver) cfd_destroy(kv.second->solver);
+    if (s->batch) cfd_batch_destroy(s->batch);
+    if (!s->opt.stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return CFD_OK;
+}
+
+}  // extern "C"

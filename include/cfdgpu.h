@@ -216,6 +216,57 @@ int cfd_batch_status(cfd_batch* b, int id, cfd_status* st);
 int cfd_batch_poll(cfd_batch* b, int cap, int* ids, int* steps, int* done, double* t, int* count);
 int cfd_batch_download(cfd_batch* b, int id, double* host, int layout);
 
+/* ---- continuous-batching server --------------------------------------------
+ * Clients submit solves from any thread; a worker thread owns the GPU and,
+ * between rounds of `ticks_per_round` steps, admits queued requests in
+ * arrival order as device memory frees up (requests that do not fit yet keep
+ * their place without blocking smaller ones), advances every admitted solve
+ * together (mixed: one cfd_batch; FP64: one cfd_solver each on the worker's
+ * stream) and hands finished grids back.  No counterpart in the reference. */
+enum { CFD_REQ_QUEUED = 0, CFD_REQ_RUNNING = 1, CFD_REQ_DONE = 2, CFD_REQ_FAILED = 3 };
+
+typedef struct cfd_server_options {
+    int precision;          /* CFD_PREC_MIXED or CFD_PREC_FP64 */
+    size_t budget_bytes;    /* device memory for resident solves; 0: budget_fraction */
+    double budget_fraction; /* of the free device memory at creation (0: 0.8) */
+    int ticks_per_round;    /* steps between admission points (0: 16) */
+    void* stream;           /* cudaStream_t for all work (NULL: the server creates one) */
+} cfd_server_options;
+
+typedef struct cfd_request_info {
+    int state;              /* CFD_REQ_* */
+    int error;
+    int steps;              /* steps the solve took */
+    double t;               /* its final simulated time */
+    double submit_s;        /* submission time since server start */
+    double queue_s;         /* submit -> admission */
+    double run_s;           /* admission -> result on the host */
+    double latency_s;       /* submit -> result on the host */
+} cfd_request_info;
+
+typedef struct cfd_server_stats {
+    int64_t completed, admitted, queued, running, max_running, rounds;
+    double cell_updates;    /* completed solves: cells x steps */
+    double busy_s, wall_s;
+    size_t used_bytes, budget_bytes;
+} cfd_server_stats;
+
+typedef struct cfd_server cfd_server;
+int cfd_server_create(const cfd_server_options* opt, cfd_server** out);
+/* Queues a solve of `steps` steps (or to cfg.T) from a ghosted AoS initial
+ * grid, which is copied; CFD_ERR_BUDGET if it can never fit. */
+int cfd_server_submit(cfd_server* s, const cfd_config* cfg, const double* ic, int steps,
+                      int64_t* id);
+/* Waits up to timeout_s (< 0: forever) for a request; on completion fills
+ * info and copies the final ghosted grid to `result` (may be NULL). */
+int cfd_server_wait(cfd_server* s, int64_t id, double timeout_s, cfd_request_info* info,
+                    double* result);
+/* Forgets a finished request (frees its host copy). */
+int cfd_server_release(cfd_server* s, int64_t id);
+int cfd_server_get_stats(cfd_server* s, cfd_server_stats* st);
+/* Stops the worker (in-flight solves are dropped) and frees everything. */
+int cfd_server_destroy(cfd_server* s);
+
 /* ---- test entry: the device flux of single faces -------------------------
  * flux_computation of the MUSCL-Hancock (or Godunov) solver
  * (headers/flux_solver_MUSCLhancock.hpp:128-227 / A: :272-376) evaluated on
