@@ -2,26 +2,34 @@
 """Headline benchmark: Gcell-updates/s of the split finite-volume update.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload euler4096]
+                    [--workload served|batch256|euler4096[_mixed]|allaire2048[_mixed]|...]
 
-A step is one full time step (x sweep + y sweep + wave-speed reduction + dt)
-over the whole grid of the workload.  The default workload is the 4096 x 4096
-Euler shock/bubble problem (gamma 1.4, 32 seeded bubbles, Mach-2 shock,
-reflective top/bottom, transmissive left/right, CFL 0.8) in the plain FP64
-form, which matches the reference to the bit.  Its state (537 MB per buffer)
-is larger than the 126 MB L2, so no flush is needed between steps.
+Default workload ("served", the configuration the headline metric is quoted
+on): a seeded Poisson stream (mean 50 requests/s) of solves, 70 % Euler
+(shock + bubbles recipe) and 30 % Allaire two-material (water shock on an air
+bubble, PVRS speeds, alpha clipped to [1e-6, 1-1e-6]), cells log-uniform in
+[128^2, 2048^2], steps uniform in [100, 2000], admitted against 80 % of the
+free HBM.  K = --steps requests are timed after W = --warmup requests.
 
-value      device-resident throughput, CUDA events on the solver's stream,
-           max over ranks (N>1 runs independent replicas: the single grid is
-           not sharded; scaling "weak").
-e2e        the same metric through the C ABI with host buffers: upload of the
-           initial grid from pinned memory, the reference-shaped host loop
-           (compute_dt -> step per step, a device->host read of the wave speeds
-           each step), download of the final grid to pinned memory.
-roofline   dominant sweep kernel: algorithmic bytes (nx*ny*nvar*8 read + write)
-           over its mean CUDA-event duration, against MEASURED_PEAKS.json.
-cpu_baseline  the reference's own CPU code (oracle/_ref, all host threads) on a
-           1024x1024 instance of the same workload for a bounded number of steps.
+  value      device-resident throughput of the mixed form on that request
+             set: every request resident in one batch, each advancing to its
+             own step count (CUDA events on the batch's stream).
+  e2e        the served run through the C ABI: requests submitted from host
+             buffers at their arrival times, continuous batching, results back
+             in host memory; cell-updates of all requests / makespan.  p50/p99
+             completion latency come from this run.
+  plain_fp64 the same served run in the plain FP64 form (bit-identical to the
+             reference), for the "mixed vs plain" comparison; l1_vs_fp64 is
+             the largest relative L1 density error of a mixed result against
+             its FP64 result.
+  roofline   the dominant mixed sweep kernel on a resident sample of the
+             requests: algorithmic bytes (cells x nvar x (4+4) B read + write)
+             over its mean CUDA-event launch time, against MEASURED_PEAKS.json.
+
+Other workloads are the single-grid and batched configurations: euler4096
+(4096^2 shock/bubbles, K steps timed), allaire2048 (2048x1024 water shock),
+each in the plain FP64 form or with _mixed, and batch256 (256 uneven Euler
+instances, 64..1024 per side, 500 steps each).
 """
 from __future__ import annotations
 
@@ -46,12 +54,20 @@ METRIC = "Gcell-updates/s + p50/p99 latency: served mixed vs plain FP64, L1 err 
 UNIT = "Gcell-updates/s"
 SEED = 20261203
 
-WORKLOADS = {
-    # name: (recipe, nx, ny, nbubbles)
-    "euler4096": ("shock_bubbles", 4096, 4096, 32),
-    "euler2048": ("shock_bubbles", 2048, 2048, 32),  # smaller case for ncu captures
+# single-grid workloads: (recipe, nx, ny, nbubbles, precision)
+SINGLE = {
+    "euler4096": ("shock_bubbles", 4096, 4096, 32, "fp64"),
+    "euler4096_mixed": ("shock_bubbles", 4096, 4096, 32, "mixed"),
+    "euler2048": ("shock_bubbles", 2048, 2048, 32, "fp64"),
+    "euler2048_mixed": ("shock_bubbles", 2048, 2048, 32, "mixed"),
+    "allaire2048": ("water_shock_air_bubble", 2048, 1024, 1, "fp64"),
+    "allaire2048_mixed": ("water_shock_air_bubble", 2048, 1024, 1, "mixed"),
+    "allaire1024_mixed": ("water_shock_air_bubble", 1024, 512, 1, "mixed"),
 }
+WORKLOADS = ["served", "batch256", *SINGLE]
 
+
+# ----------------------------------------------------------------- helpers --
 
 def _peaks() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
@@ -64,7 +80,7 @@ def _peaks() -> tuple[float, str]:
 
 
 def _profile_traffic(kernel: str) -> float | None:
-    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    """DRAM bytes per launch of `kernel` from the committed ncu summaries."""
     for f in sorted((ROOT / "profiles").glob("*.md")):
         m = re.search(rf"traffic_bytes_per_launch\[{re.escape(kernel)}\]\s*[:=]\s*([0-9.eE+]+)",
                       f.read_text())
@@ -137,121 +153,474 @@ def _gpu_id(torch, dev: int) -> str | None:
         return None
 
 
-def cpu_baseline(recipe: str, nbub: int, budget_s: float = 15.0) -> dict:
-    """The reference's own CPU path (oracle/_ref, all host threads) on a
-    1024 x 1024 instance of the workload, steps bounded to ~budget_s."""
+def _rel_l1_density(a: np.ndarray, b: np.ndarray, model: int) -> float:
+    ra = a[2:-2, 2:-2, 0] if model == 0 else a[2:-2, 2:-2, 0] + a[2:-2, 2:-2, 1]
+    rb = b[2:-2, 2:-2, 0] if model == 0 else b[2:-2, 2:-2, 0] + b[2:-2, 2:-2, 1]
+    return float(np.abs(ra - rb).sum() / np.abs(rb).sum())
+
+
+# ------------------------------------------------------- request streams --
+
+def served_requests(n: int, seed: int):
+    """The served mix: (arrival_s, recipe, nx, ny, steps, seed, nbubbles)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(n):
+        t += rng.exponential(1.0 / 50.0)
+        euler = rng.uniform() < 0.7
+        cells = math.exp(rng.uniform(math.log(128 ** 2), math.log(2048 ** 2)))
+        steps = int(rng.integers(100, 2001))
+        if euler:
+            nx = ny = max(16, int(round(math.sqrt(cells))))
+            out.append((t, "shock_bubbles", nx, ny, steps, seed + k, int(rng.integers(4, 33))))
+        else:
+            ny = max(16, int(round(math.sqrt(cells / 2))))
+            out.append((t, "water_shock_air_bubble", 2 * ny, ny, steps, seed + k, 1))
+    return out
+
+
+def batch_instances(n: int, seed: int):
+    """Batched config: Euler instances with nx, ny log-uniform in [64, 1024]
+    and 4-16 bubbles each, 500 steps."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nx = int(round(math.exp(rng.uniform(math.log(64), math.log(1024)))))
+        ny = int(round(math.exp(rng.uniform(math.log(64), math.log(1024)))))
+        out.append(("shock_bubbles", nx, ny, 500, seed + k, int(rng.integers(4, 17))))
+    return out
+
+
+def build_ic(G, recipe, nx, ny, seed, nbub):
+    cfg = G.recipe_config(recipe, nx, ny)
+    return cfg, G.recipe_ic(cfg, recipe, seed=seed, nbubbles=nbub)
+
+
+# ------------------------------------------------------------ CPU baseline --
+
+def _ref_rate(O, G, recipe, n_x, n_y, nbub, budget_s, cores):
+    import ctypes
+
+    model = "euler" if recipe == "shock_bubbles" else "allaire"
+    cfg, ic = build_ic(G, recipe, n_x, n_y, SEED, nbub)
+    p = O.make_params(n_x, n_y, cfg.dx, cfg.dy, cfg.gamma1, cfg.pinf1, cfg.gamma2, cfg.pinf2,
+                      bc=tuple(cfg.bc), cfl=cfg.cfl, T=cfg.T, limiter=cfg.limiter,
+                      wavespeed=cfg.wavespeed, z_min=cfg.z_min)
+    lib = O.ref_lib(model)
+    f = getattr(lib, f"ref_{model}_last_loop_seconds")
+    f.restype = ctypes.c_double
+    g = ic.copy()
+    O.ref_run(model, p, g, 1, threads=cores)
+    t1 = f()
+    steps = max(2, min(60, int(budget_s / max(t1, 1e-3))))
+    taken, _, _, _ = O.ref_run(model, p, g, steps, n=1, threads=cores)
+    return n_x * n_y * taken, f(), taken
+
+
+def cpu_baseline(workload: str, budget_s: float = 16.0) -> dict:
+    """The reference's own CPU code (oracle/_ref, all host threads) on a
+    bounded sample of the workload."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import cfdgpu as G
     import oracle_py as O
 
-    if not O.ref_available("euler"):
-        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                "sample": "unavailable: oracle/_ref/libref_euler.so not built"}
     cores = os.cpu_count() or 1
-    n = 1024
-    cfg = G.recipe_config(recipe, n, n)
-    ic = G.recipe_ic(cfg, recipe, seed=SEED, nbubbles=nbub)
-    p = O.make_params(n, n, cfg.dx, cfg.dy, cfg.gamma1, cfg.pinf1, bc=tuple(cfg.bc), cfl=cfg.cfl,
-                      T=cfg.T, limiter=cfg.limiter)
-    lib = O.ref_lib("euler")
-    lib.ref_euler_last_loop_seconds.restype = __import__("ctypes").c_double
-    g = ic.copy()
-    O.ref_run("euler", p, g, 1, threads=cores)  # first step: calibrate
-    t1 = lib.ref_euler_last_loop_seconds()
-    steps = max(2, min(50, int(budget_s / max(t1, 1e-3))))
-    taken, nn, tt, _ = O.ref_run("euler", p, g, steps, n=1, t=0.0, threads=cores)
-    sec = lib.ref_euler_last_loop_seconds()
-    val = n * n * taken / sec / 1e9
-    return {"value": val, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"{n}x{n} shock-bubble grid (same recipe), {taken} steps, "
-                      f"{cores} OpenMP threads, time loop only ({sec:.1f} s)"}
+    if not (O.ref_available("euler") and O.ref_available("allaire")):
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref (reference build) absent"}
+    parts = []
+    if workload in ("served", "batch256") or workload.startswith("euler"):
+        parts.append(("shock_bubbles", 1024, 1024, 32, 0.7 if workload == "served" else 1.0))
+    if workload == "served" or workload.startswith("allaire"):
+        parts.append(("water_shock_air_bubble", 512, 256, 1, 0.3 if workload == "served" else 1.0))
+    cells = secs = 0.0
+    desc = []
+    for recipe, nx, ny, nb, share in parts:
+        c, s, k = _ref_rate(O, G, recipe, nx, ny, nb, budget_s * share, cores)
+        cells += c
+        secs += s
+        desc.append(f"{recipe} {nx}x{ny} x {k} steps")
+    return {"value": cells / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": "; ".join(desc) + f" ({cores} OpenMP threads, time loop only, {secs:.1f} s)"}
 
 
 def run_reference(args) -> None:
-    """Reference arm: the reference's CPU implementation on a bounded sample
-    of the workload (512 x 512 instance, one time step per step)."""
+    """Reference arm: the reference's CPU implementation (oracle/_ref: its
+    own sources built here) on a bounded sample of the workload, one time
+    step per bench step, all host threads."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle_py as O
-
-    recipe, nx, ny, nbub = WORKLOADS[args.workload]
-    base = {"impl": "reference", "metric": METRIC, "unit": UNIT}
-    if not O.ref_available("euler"):
-        print(json.dumps({**base, "unavailable": "oracle/_ref/libref_euler.so (reference build) absent"}))
-        return
     import ctypes
 
+    import oracle_py as O
+
+    base = {"impl": "reference", "metric": METRIC, "unit": UNIT}
+    if not (O.ref_available("euler") and O.ref_available("allaire")):
+        print(json.dumps({**base, "unavailable": "oracle/_ref (reference build) absent"}))
+        return
     import cfdgpu as G
 
     cores = os.cpu_count() or 1
-    n = 512
-    cfg = G.recipe_config(recipe, n, n)
-    ic = G.recipe_ic(cfg, recipe, seed=SEED, nbubbles=nbub)
-    p = O.make_params(n, n, cfg.dx, cfg.dy, cfg.gamma1, cfg.pinf1, bc=tuple(cfg.bc), cfl=cfg.cfl,
-                      T=cfg.T, limiter=cfg.limiter)
-    lib = O.ref_lib("euler")
-    lib.ref_euler_last_loop_seconds.restype = ctypes.c_double
-    g = ic.copy()
-    if args.warmup:
-        O.ref_run("euler", p, g, args.warmup, threads=cores)
-    taken, nn, tt, _ = O.ref_run("euler", p, g, args.steps, n=args.warmup, t=0.0, threads=cores)
-    sec = lib.ref_euler_last_loop_seconds()
-    val = n * n * taken / sec / 1e9
-    sample = (f"{n}x{n} instance of the {nx}x{ny} shock-bubble workload, one time step per step, "
-              f"{cores} OpenMP threads")
+    w = args.workload
+    parts = []
+    if w in ("served", "batch256") or w.startswith("euler"):
+        parts.append(("euler", "shock_bubbles", 512, 512, 32))
+    if w == "served" or w.startswith("allaire"):
+        parts.append(("allaire", "water_shock_air_bubble", 256, 128, 1))
+    cells = secs = 0.0
+    for model, recipe, nx, ny, nb in parts:
+        cfg, ic = build_ic(G, recipe, nx, ny, SEED, nb)
+        p = O.make_params(nx, ny, cfg.dx, cfg.dy, cfg.gamma1, cfg.pinf1, cfg.gamma2, cfg.pinf2,
+                          bc=tuple(cfg.bc), cfl=cfg.cfl, T=cfg.T, limiter=cfg.limiter,
+                          wavespeed=cfg.wavespeed, z_min=cfg.z_min)
+        f = getattr(O.ref_lib(model), f"ref_{model}_last_loop_seconds")
+        f.restype = ctypes.c_double
+        g = ic.copy()
+        if args.warmup:
+            O.ref_run(model, p, g, args.warmup, threads=cores)
+        taken, _, _, _ = O.ref_run(model, p, g, args.steps, n=args.warmup, threads=cores)
+        cells += nx * ny * taken
+        secs += f()
+    val = cells / secs / 1e9
+    sample = (" + ".join(f"{r} {nx}x{ny}" for _, r, nx, ny, _ in parts) +
+              f", {args.steps} steps each, {cores} OpenMP threads, time loop only")
     print(json.dumps({
-        **base, "value": val, "n_gpus": args.gpus, "steps": taken, "warmup": args.warmup,
-        "ms_per_step": 1e3 * sec / max(taken, 1), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "grid": [n, n], "model": "euler",
-                   "precision": "fp64", "sample_of": [nx, ny]},
+        **base, "value": val, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * secs / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w, "sample": sample},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
 
-def end_to_end(G, torch, cfg, ic, K, W, barrier, max_over_ranks, world, cells) -> dict:
-    """Same metric through the C ABI with host buffers: upload from pinned
-    memory, the reference-shaped host loop (compute_dt -> step), download."""
-    pinned_ic = torch.empty(ic.size, dtype=torch.float64, pin_memory=True)
-    pinned_ic.numpy()[:] = ic.ravel()
-    ic_pinned = pinned_ic.numpy().reshape(ic.shape)
-    pinned_out = torch.empty(ic.size, dtype=torch.float64, pin_memory=True)
-    out_pinned = pinned_out.numpy().reshape(ic.shape)
-    s2 = G.Solver(cfg)
-    s2.upload(ic_pinned)
-    s2.run_reference_loop(W)
-    s2.download(out=out_pinned)
-    barrier()
+# ---------------------------------------------------------------- GPU arms --
+
+class Ctx:
+    def __init__(self, torch, dist, world, rank, local):
+        self.torch, self.dist, self.world, self.rank, self.local = torch, dist, world, rank, local
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([x], device="cuda", dtype=self.torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([x], device="cuda", dtype=self.torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+
+def roofline(kernel: str, ms: float, launches: int, bytes_per_launch: float, traffic_key: str):
+    peak, kind = _peaks()
+    avg_s = ms / max(launches, 1) / 1e3
+    achieved = bytes_per_launch / avg_s / 1e9 if avg_s > 0 else 0.0
+    return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
+            "peak_kind": kind, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": _profile_traffic(traffic_key),
+            "algorithmic_bytes_per_launch": bytes_per_launch, "mean_launch_ms": avg_s * 1e3}
+
+
+def bench_single(args, ctx, G, stream, clocks):
+    torch = ctx.torch
+    recipe, nx, ny, nbub, prec = SINGLE[args.workload]
+    cfg, ic = build_ic(G, recipe, nx, ny, SEED + ctx.rank, nbub)
+    cfg.stream = stream.cuda_stream
+    cells, nv, K, W = nx * ny, cfg.nvar, args.steps, args.warmup
+    model = "euler" if cfg.model == G.EULER else "allaire"
+    if prec == "fp64":
+        s = G.Solver(cfg)
+        s.upload(ic)
+        s.advance(W)
+        s.synchronize()
+        s.set_kernel_timing(True)
+        s.reset_kernel_times()
+        run = lambda: s.advance(K)
+    else:
+        s = G.Batch(stream=stream.cuda_stream)
+        mid = s.add(cfg, ic, 0)
+        s.autotune(1)
+        s.step(W)
+        torch.cuda.synchronize()
+        run = lambda: s.step(K)
+    clocks.start()
+    time.sleep(0.3)
+    ctx.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.barrier()
+    ck = clocks.stop()
+    ms = ctx.max(e0.elapsed_time(e1))
+    if prec == "fp64":
+        kms, kn = s.kernel_times()
+        st = s.status()
+        launches = kn[0] + kn[1]
+        dom = 0 if kms[0] >= kms[1] else 1
+        rl = roofline(["sweep_x", "sweep_y"][dom], kms[dom], kn[dom], cells * nv * 8 * 2,
+                      f"{model}_sweep_{'xy'[dom]}")
+    else:
+        mx, my, n = s.step_timed(4)
+        st = s.status(mid)
+        launches = 2 * K
+        dom = 0 if mx >= my else 1
+        rl = roofline(["mixed_sweep_x", "mixed_sweep_y"][dom], [mx, my][dom], 4,
+                      cells * nv * 8 * 2, f"{model}_mixed_sweep_{'xy'[dom]}")
+    s.close()
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_single(G, torch, cfg, ic, K, W, ctx, prec)
+    value = ctx.world * cells * K / (ms / 1e3) / 1e9
+    config = {"workload": args.workload, "model": model, "precision": prec, "grid": [nx, ny],
+              "bubbles": nbub, "seed": SEED, "cfl": cfg.cfl,
+              "l2": f"state {cells * nv * 8 / 1e6:.0f} MB per buffer vs 126 MB L2"
+                    + (", no flush" if cells * nv * 8 > 126e6 else ""),
+              "parallelism": f"replicas x{ctx.world}"}
+    return {"value": value, "ms_per_step": ms / K,
+            "dtype": "f64" if prec == "fp64" else "f32+f32comp", "config": config, "clocks": ck,
+            "gpu_launches": launches, "roofline": rl, "e2e": e2e, "sim": {"n": st.n, "t": st.t}}
+
+
+def e2e_single(G, torch, cfg, ic, K, W, ctx, prec) -> dict:
+    """Same metric through the C ABI with pinned host buffers: upload, K
+    steps (FP64: the reference-shaped compute_dt -> step loop), download."""
+    pin_in = torch.empty(ic.size, dtype=torch.float64, pin_memory=True).numpy().reshape(ic.shape)
+    pin_in[:] = ic
+    pin_out = torch.empty(ic.size, dtype=torch.float64, pin_memory=True).numpy().reshape(ic.shape)
+    ctx.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    s2.upload(ic_pinned)
-    taken, n2, t2 = s2.run_reference_loop(K)
-    s2.download(out=out_pinned)
+    if prec == "fp64":
+        s = G.Solver(cfg)
+        s.upload(pin_in)
+        taken, _, _ = s.run_reference_loop(K)
+        s.download(out=pin_out)
+        d2h_step = 96
+    else:
+        s = G.Batch(stream=cfg.stream)
+        mid = s.add(cfg, pin_in, 0)
+        s.step(K)
+        pin_out[:] = s.download(mid)
+        taken = K
+        d2h_step = 0
     torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    s2.close()
-    state_bytes = ic.size * 8
-    status_bytes = 96  # DevState read by compute_dt
-    return {"value": world * cells * taken / e2e_s / 1e9, "unit": UNIT,
-            "h2d_bytes_per_step": state_bytes / K,
-            "d2h_bytes_per_step": status_bytes + state_bytes / K, "seconds": e2e_s}
+    secs = ctx.max(time.perf_counter() - t0)
+    s.close()
+    cells = cfg.nx * cfg.ny
+    return {"value": ctx.world * cells * taken / secs / 1e9, "unit": UNIT,
+            "h2d_bytes_per_step": ic.size * 8 / K, "d2h_bytes_per_step": d2h_step + ic.size * 8 / K,
+            "seconds": secs}
+
+
+def bench_batch(args, ctx, G, stream, clocks):
+    torch = ctx.torch
+    insts = batch_instances(256, SEED + 1000 * ctx.rank)
+    ics = [build_ic(G, r, nx, ny, sd, nb) for r, nx, ny, steps, sd, nb in insts]
+    cells = sum(c.nx * c.ny for c, _ in ics)
+    K, W = args.steps, args.warmup
+    b = G.Batch(stream=stream.cuda_stream)
+    for (c, ic), inst in zip(ics, insts):
+        b.add(c, ic, inst[3])
+    tune_ms = b.autotune(1)
+    pre = {i: s for i, s, _, _ in b.poll()}
+    b.step(W)
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    ctx.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start = {i: s for i, s, _, _ in b.poll()}
+    e0.record(stream)
+    b.step(K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.barrier()
+    ck = clocks.stop()
+    ms = ctx.max(e0.elapsed_time(e1))
+    end = {i: s for i, s, _, _ in b.poll()}
+    upd = sum(b.cfgs[i].nx * b.cfgs[i].ny * (end[i] - start[i]) for i in end)
+    mx, my, n = b.step_timed(4)
+    dom = 0 if mx >= my else 1
+    rl = roofline(["mixed_sweep_x", "mixed_sweep_y"][dom], [mx, my][dom], 4, cells * 4 * 8 * 2,
+                  f"batch_mixed_sweep_{'xy'[dom]}")
+    shapes = b.get_shapes(0)
+    b.close()
+    value = ctx.sum(upd) / (ms / 1e3) / 1e9
+    e2e = None
+    if not args.no_e2e:
+        ctx.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b2 = G.Batch(stream=stream.cuda_stream)
+        ids = [b2.add(c, ic, inst[3]) for (c, ic), inst in zip(ics, insts)]
+        b2.step(K)
+        outs = [b2.download(i) for i in ids]
+        torch.cuda.synchronize()
+        secs = ctx.max(time.perf_counter() - t0)
+        b2.close()
+        upd2 = sum(c.nx * c.ny * min(i[3], K) for (c, _), i in zip(ics, insts))
+        nbytes = sum(ic.size * 8 for _, ic in ics)
+        e2e = {"value": ctx.sum(upd2) / secs / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": nbytes / K, "d2h_bytes_per_step": nbytes / K, "seconds": secs}
+        del outs
+    return {"value": value, "ms_per_step": ms / K, "dtype": "f32+f32comp",
+            "config": {"workload": "batch256", "model": "euler", "precision": "mixed",
+                       "instances": 256, "cells": cells, "sizes": "nx, ny log-uniform [64, 1024]",
+                       "bubbles": "4-16 per instance", "steps_per_instance": 500,
+                       "tile_shapes": list(shapes), "autotune_tick_ms": tune_ms,
+                       "autotune_steps": sum(pre.values()), "graph": "8 ticks per CUDA graph",
+                       "l2": f"state {cells * 32 / 1e6:.0f} MB > 126 MB L2, no flush",
+                       "parallelism": f"replicas x{ctx.world}"},
+            "clocks": ck, "gpu_launches": 2 * K, "roofline": rl, "e2e": e2e,
+            "sim": {"cell_updates_timed": upd}}
+
+
+def _serve(G, reqs, ics, precision, ticks, stream):
+    """Submits the requests at their arrival times; returns per-request
+    (info, result), server statistics and the makespan."""
+    srv = G.Server(precision, budget_fraction=0.8, ticks_per_round=ticks,
+                   stream=stream.cuda_stream if stream is not None else None)
+    ids = [None] * len(reqs)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for k, r in enumerate(reqs):
+            delay = r[0] - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            cfg, ic = ics[k]
+            ids[k] = srv.submit(cfg, ic, r[4])
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    res = [srv.wait(i) for i in ids]
+    makespan = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    return res, st, makespan
+
+
+def bench_served(args, ctx, G, stream, clocks):
+    torch = ctx.torch
+    K, W = max(args.steps, 4), args.warmup
+    reqs = served_requests(W + K, SEED + 7919 * ctx.rank)
+    t_ic = time.perf_counter()
+    ics = [build_ic(G, rec, nx, ny, sd, nb) for (_, rec, nx, ny, steps, sd, nb) in reqs]
+    t_ic = time.perf_counter() - t_ic
+    warm, timed = reqs[:W], reqs[W:]
+    warm_ics, timed_ics = ics[:W], ics[W:]
+    base = timed[0][0]
+    timed = [(r[0] - base, *r[1:]) for r in timed]
+    upd = sum(r[2] * r[3] * r[4] for r in timed)
+    if warm:
+        _serve(G, [(0.0, *r[1:]) for r in warm], warm_ics, G.MIXED, 16, stream)
+
+    # device-resident throughput of the mixed form on the timed request set
+    b = G.Batch(stream=stream.cuda_stream)
+    ids = [b.add(c, ic, r[4]) for (c, ic), r in zip(timed_ics, timed)]
+    b.autotune(1)  # trial steps are real steps; they are not counted below
+    before = {i: s for i, s, _, _ in b.poll()}
+    max_steps = max(r[4] for r in timed)
+    clocks.start()
+    time.sleep(0.3)
+    ctx.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(max_steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = ctx.max(e0.elapsed_time(e1))
+    res_upd = sum(b.cfgs[i].nx * b.cfgs[i].ny * (r[4] - before[i]) for i, r in zip(ids, timed))
+    value = ctx.sum(res_upd) / (ms / 1e3) / 1e9
+    b.close()
+    # roofline of the mixed sweeps on a resident sample (16 requests)
+    b = G.Batch(stream=stream.cuda_stream)
+    sample = list(zip(timed_ics, timed))[:16]
+    for (c, ic), r in sample:
+        b.add(c, ic, r[4])
+    b.step(2)
+    mx, my, _n = b.step_timed(4)
+    b.close()
+    dom = 0 if mx >= my else 1
+    byts = sum(c.nx * c.ny * c.nvar * 8 * 2 for (c, _), _r in sample)
+    rl = roofline(["mixed_sweep_x", "mixed_sweep_y"][dom], [mx, my][dom], 4, byts,
+                  f"served_mixed_sweep_{'xy'[dom]}")
+    rl["note"] = ("16-request resident sample, one launch per model and direction per tick; "
+                  "bytes summed over the requests of a tick, time summed over its launches")
+
+    # served runs (host buffers, arrivals, continuous batching)
+    ctx.barrier()
+    res_m, st_m, mk_m = _serve(G, timed, timed_ics, G.MIXED, 16, stream)
+    res_f, st_f, mk_f = _serve(G, timed, timed_ics, G.FP64, 16, stream)
+    lat_m = [i.latency_s for i, _ in res_m]
+    lat_f = [i.latency_s for i, _ in res_f]
+    pct = lambda v, q: float(np.percentile(v, q))
+    l1 = [_rel_l1_density(a, f, c.model) for (_, a), (_, f), (c, _) in zip(res_m, res_f, timed_ics)]
+    nbytes = sum(ic.size * 8 for _, ic in timed_ics)
+    e2e_val = ctx.sum(upd) / ctx.max(mk_m) / 1e9
+    fp64_val = ctx.sum(upd) / ctx.max(mk_f) / 1e9
+    models = 1 + any(r[1] != "shock_bubbles" for r in timed)
+    return {
+        "value": value, "ms_per_step": ms / max_steps, "dtype": "f32+f32comp",
+        "config": {"workload": "served", "requests": len(timed), "warmup_requests": W,
+                   "arrivals": "Poisson, mean 50/s, seeded",
+                   "mix": "70% Euler shock_bubbles, 30% Allaire water_shock_air_bubble "
+                          "(PVRS, alpha clip 1e-6)",
+                   "cells": "log-uniform [128^2, 2048^2]", "steps": "uniform [100, 2000]",
+                   "budget": "80% of free HBM", "ticks_per_round": 16, "seed": SEED,
+                   "cell_updates": upd, "ic_build_s": t_ic,
+                   "value_def": "all timed requests resident in one batch, device time",
+                   "l2": "resident set >> 126 MB L2, no flush",
+                   "parallelism": f"replicas x{ctx.world}"},
+        "p50_ms": 1e3 * pct(lat_m, 50), "p99_ms": 1e3 * pct(lat_m, 99),
+        "plain_fp64": {"value": fp64_val, "unit": UNIT, "p50_ms": 1e3 * pct(lat_f, 50),
+                       "p99_ms": 1e3 * pct(lat_f, 99), "makespan_s": mk_f,
+                       "device_s": st_f.device_s, "max_resident": st_f.max_running},
+        "mixed_vs_plain": e2e_val / fp64_val,
+        "l1_vs_fp64": {"max": max(l1), "median": float(np.median(l1)), "bound": 1e-4},
+        "clocks": ck, "gpu_launches": 2 * models * max_steps,
+        "roofline": rl,
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes / len(timed),
+                "d2h_bytes_per_step": nbytes / len(timed), "step": "one request",
+                "makespan_s": mk_m, "device_s": st_m.device_s, "max_resident": st_m.max_running},
+        "sim": {"max_steps": max_steps},
+    }
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="euler4096", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="served", choices=WORKLOADS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling)")
     args = ap.parse_args()
-    if args.warmup < 3 and args.impl == "ours":
+    if args.steps is None:
+        args.steps = 48 if args.workload == "served" else 50
+    if args.warmup is None:
+        args.warmup = 4 if args.workload == "served" else 5
+    if args.impl == "ours" and args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
@@ -269,96 +638,27 @@ def main() -> None:
     if world > 1:
         import datetime
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    recipe, nx, ny, nbub = WORKLOADS[args.workload]
-    cfg = G.recipe_config(recipe, nx, ny)
-    ic = G.recipe_ic(cfg, recipe, seed=SEED + rank, nbubbles=nbub)
-    stream = torch.cuda.Stream()  # a real stream: the library must not fall back to its own
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    ctx = Ctx(torch, dist, world, rank, local)
+    stream = torch.cuda.Stream()  # a real stream: the library runs on it
     torch.cuda.set_stream(stream)
-    cfg.stream = stream.cuda_stream
-    cells = nx * ny
-    nv = cfg.nvar
-    K, W = args.steps, args.warmup
-
-    # ---- device-resident throughput --------------------------------------
-    s = G.Solver(cfg)
-    s.upload(ic)
-    s.advance(W)
-    s.synchronize()
-    s.set_kernel_timing(True)
-    s.reset_kernel_times()
     clocks = ClockSampler(_gpu_id(torch, local))
-    clocks.start()
-    time.sleep(0.3)
-    barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    s.advance(K)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    kms, kn = s.kernel_times()
-    st = s.status()
-    s.set_kernel_timing(False)
-    ms_max = max_over_ranks(ms)
-    value = world * cells * K / (ms_max / 1e3) / 1e9
-
-    # ---- roofline of the dominant sweep ----------------------------------
-    peak, peak_kind = _peaks()
-    dom = 0 if kms[0] >= kms[1] else 1
-    kname = ["sweep_x", "sweep_y"][dom]
-    avg_s = kms[dom] / max(kn[dom], 1) / 1e3
-    bytes_launch = cells * nv * 8 * 2
-    achieved = bytes_launch / avg_s / 1e9
-    traffic = _profile_traffic(f"euler_{kname}")
-
-    # ---- end to end through the C ABI with host buffers ------------------
-    e2e = None
-    if not args.no_e2e:
-        e2e = end_to_end(G, torch, cfg, ic, K, W, barrier, max_over_ranks, world, cells)
-    s.close()
-    
+    if args.workload == "served":
+        r = bench_served(args, ctx, G, stream, clocks)
+    elif args.workload == "batch256":
+        r = bench_batch(args, ctx, G, stream, clocks)
+    else:
+        r = bench_single(args, ctx, G, stream, clocks)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(recipe, nbub)
-
+        cpu = cpu_baseline(args.workload)
     if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
-            "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "model": "euler", "precision": "fp64 (plain)",
-                       "grid": [nx, ny], "bubbles": nbub, "seed": SEED, "cfl": cfg.cfl,
-                       "limiter": "minmod", "flux": "MUSCL-Hancock + HLLC",
-                       "splitting": "naive", "l2": "state 537 MB/buffer > 126 MB L2, no flush",
-                       "parallelism": f"replicas x{world}"},
-            "clocks": ck,
-            "gpu_launches": int(kn[0] + kn[1]),
-            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic,
-                         "algorithmic_bytes_per_launch": bytes_launch,
-                         "mean_launch_ms": [kms[0] / max(kn[0], 1), kms[1] / max(kn[1], 1)]},
-            "e2e": e2e,
-            "cpu_baseline": cpu,
-            "sim": {"n": st.n, "t": st.t, "counters": st.counter_dict()},
-        }
+        line = {"metric": METRIC, "value": r.pop("value"), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r.pop("ms_per_step"),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": r.pop("dtype"), "data": "synthetic", "config": r.pop("config")}
+        line.update(r)
+        line["cpu_baseline"] = cpu
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

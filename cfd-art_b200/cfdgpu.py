@@ -93,7 +93,7 @@ class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_int64), ("admitted", C.c_int64), ("queued", C.c_int64),
                 ("running", C.c_int64), ("max_running", C.c_int64), ("rounds", C.c_int64),
                 ("cell_updates", C.c_double), ("busy_s", C.c_double), ("wall_s", C.c_double),
-                ("used_bytes", C.c_size_t), ("budget_bytes", C.c_size_t)]
+                ("device_s", C.c_double), ("used_bytes", C.c_size_t), ("budget_bytes", C.c_size_t)]
 
 
 REQ_DONE, REQ_FAILED = 2, 3

@@ -72,6 +72,8 @@ struct cfd_server {
     // statistics
     double cell_updates = 0.0;
     double busy_s = 0.0;
+    double device_s = 0.0;   // CUDA-event time of the step rounds
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int64_t completed = 0, rounds = 0, admitted = 0;
     int max_running = 0;
     int worker_error = 0;
@@ -161,6 +163,7 @@ void worker_main(cfd_server* s) {
         if (run.empty()) continue;
         auto tr = Clock::now();
         // one round of batched steps
+        cudaEventRecord(s->ev0, s->stream);
         if (s->opt.precision == CFD_PREC_MIXED) {
             if (cfd_batch_step(s->batch, K)) s->worker_error = CFD_ERR_CUDA;
         } else {
@@ -169,6 +172,7 @@ void worker_main(cfd_server* s) {
                 if (k > 0 && cfd_advance(r->solver, k) == CFD_OK) r->issued += k;
             }
         }
+        cudaEventRecord(s->ev1, s->stream);
         // completion check: one status read per member
         std::vector<Request*> done;
         for (Request* r : run) {
@@ -194,9 +198,13 @@ void worker_main(cfd_server* s) {
             s->running.erase(std::find(s->running.begin(), s->running.end(), r->id));
             finish(s, r, rc);
         }
+        float dev_ms = 0.f;
+        cudaEventSynchronize(s->ev1);
+        cudaEventElapsedTime(&dev_ms, s->ev0, s->ev1);
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->busy_s += secs(tr, Clock::now());
+            s->device_s += 1e-3 * dev_ms;
             s->rounds++;
         }
         if (!done.empty()) s->cv_done.notify_all();
@@ -232,6 +240,8 @@ int cfd_server_create(const cfd_server_options* opt, cfd_server** out) {
             return rc;
         }
     }
+    cudaEventCreate(&s->ev0);
+    cudaEventCreate(&s->ev1);
     s->t0 = Clock::now();
     s->worker = std::thread(worker_main, s);
     *out = s;
@@ -318,6 +328,7 @@ int cfd_server_get_stats(cfd_server* s, cfd_server_stats* st) {
     st->rounds = s->rounds;
     st->cell_updates = s->cell_updates;
     st->busy_s = s->busy_s;
+    st->device_s = s->device_s;
     st->wall_s = secs(s->t0, Clock::now());
     st->used_bytes = s->used;
     st->budget_bytes = s->budget;
@@ -335,6 +346,8 @@ int cfd_server_destroy(cfd_server* s) {
     for (auto& kv : s->reqs)
         if (kv.second->solver) cfd_destroy(kv.second->solver);
     if (s->batch) cfd_batch_destroy(s->batch);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
     if (!s->opt.stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return CFD_OK;

@@ -247,7 +247,8 @@ typedef struct cfd_request_info {
 typedef struct cfd_server_stats {
     int64_t completed, admitted, queued, running, max_running, rounds;
     double cell_updates;    /* completed solves: cells x steps */
-    double busy_s, wall_s;
+    double busy_s, wall_s;  /* worker time in step rounds; time since creation */
+    double device_s;        /* CUDA-event time of the step rounds */
     size_t used_bytes, budget_bytes;
 } cfd_server_stats;
 
