@@ -64,7 +64,10 @@ int launch_t(const MixedArgs& a, int sms, cudaStream_t st) {
         if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     }
     int grid = std::max(1, std::min(a.ntiles, per_sm * sms));
-    mixed_sweep_kernel<MODEL, DIR, TS, NA><<<grid, 256, smem, st>>>(a);
+    MixedArgs b = a;
+    b.chunk = (a.ntiles + grid - 1) / grid;
+    grid = (a.ntiles + b.chunk - 1) / b.chunk;
+    mixed_sweep_kernel<MODEL, DIR, TS, NA><<<grid, 256, smem, st>>>(b);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "mixed sweep launch: %s", cudaGetErrorString(e));
     return CFD_OK;
@@ -93,28 +96,38 @@ int tiles_for(int nx, int ny, int dir, Shape s) {
 
 // ---- conversion kernels ----------------------------------------------------
 
-__global__ void ghosted_to_mixed(const double* __restrict__ src, float* __restrict__ hi,
-                                 float* __restrict__ lo, double* __restrict__ soa, int nx, int ny,
-                                 int g, int nv, int pitch, long long plane) {
-    long long n = (long long)nx * ny;
+// Ghosted FP64 AoS grid -> packed value/compensation planes, plus an FP64
+// SoA copy for the initial wave-speed reduction.
+__global__ void ghosted_to_mixed(const double* __restrict__ src, Inst I,
+                                 double* __restrict__ soa, int g) {
+    long long n = (long long)I.nx * I.ny;
+    const int nv = I.nv;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
          idx += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(idx / nx), j = (int)(idx % nx);
-        const double* c = src + ((long long)(i + g) * (nx + 2 * g) + (j + g)) * nv;
-        long long o = (long long)i * pitch + j;
+        int i = (int)(idx / I.nx), j = (int)(idx % I.nx);
+        const double* c = src + ((long long)(i + g) * (I.nx + 2 * g) + (j + g)) * nv;
+        long long o = (long long)i * I.pitch + j;
+        float h[6], l[6];
         for (int k = 0; k < nv; ++k) {
             double x = c[k];
-            float h = (float)x;
-            hi[k * plane + o] = h;
-            lo[k * plane + o] = (float)(x - (double)h);
-            soa[k * plane + o] = x;
+            h[k] = (float)x;
+            l[k] = (float)(x - (double)h[k]);
+            soa[k * I.plane + o] = x;
+        }
+        I.q4[0][0][o] = make_float4(h[0], h[1], h[2], h[3]);
+        I.q4[0][1][o] = make_float4(l[0], l[1], l[2], l[3]);
+        if (nv == 6) {
+            I.q2[0][0][o] = make_float2(h[4], h[5]);
+            I.q2[0][1][o] = make_float2(l[4], l[5]);
         }
     }
 }
 
-__global__ void mixed_to_ghosted(const float* __restrict__ hi, const float* __restrict__ lo,
-                                 double* __restrict__ dst, int nx, int ny, int g, int nv, int pitch,
-                                 long long plane, int bcL, int bcR, int bcB, int bcT, int im, int it) {
+// Packed planes of buffer `buf` -> FP64 AoS with the boundary mirror in the
+// ghost strips (g = 0: interior only); corners are zero.
+__global__ void mixed_to_ghosted(Inst I, int buf, double* __restrict__ dst, int g, int im,
+                                 int it, int use_bc) {
+    const int nx = I.nx, ny = I.ny, nv = I.nv;
     int W = nx + 2 * g, H = ny + 2 * g;
     long long n = (long long)W * H;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
@@ -128,15 +141,20 @@ __global__ void mixed_to_ghosted(const float* __restrict__ hi, const float* __re
             continue;
         }
         int si = i, sj = j, neg = -1;
-        if (j < 0) { sj = -j - 1; if (bcL) neg = im; }
-        else if (j >= nx) { sj = 2 * nx - 1 - j; if (bcR) neg = im; }
-        if (i < 0) { si = -i - 1; if (bcB) neg = it; }
-        else if (i >= ny) { si = 2 * ny - 1 - i; if (bcT) neg = it; }
-        long long o = (long long)si * pitch + sj;
-        for (int k = 0; k < nv; ++k) {
-            double v = (double)hi[k * plane + o] + (double)lo[k * plane + o];
-            d[k] = (k == neg) ? -v : v;
+        if (j < 0) { sj = -j - 1; if (use_bc && I.bc[0]) neg = im; }
+        else if (j >= nx) { sj = 2 * nx - 1 - j; if (use_bc && I.bc[1]) neg = im; }
+        if (i < 0) { si = -i - 1; if (use_bc && I.bc[2]) neg = it; }
+        else if (i >= ny) { si = 2 * ny - 1 - i; if (use_bc && I.bc[3]) neg = it; }
+        long long o = (long long)si * I.pitch + sj;
+        float4 a = I.q4[buf][0][o], b = I.q4[buf][1][o];
+        double v[6] = {(double)a.x + b.x, (double)a.y + b.y, (double)a.z + b.z, (double)a.w + b.w,
+                       0.0, 0.0};
+        if (nv == 6) {
+            float2 c = I.q2[buf][0][o], e = I.q2[buf][1][o];
+            v[4] = (double)c.x + e.x;
+            v[5] = (double)c.y + e.y;
         }
+        for (int k = 0; k < nv; ++k) d[k] = (k == neg) ? -v[k] : v[k];
     }
 }
 
@@ -354,7 +372,7 @@ size_t member_bytes(const cfd_config& c, size_t* plane_out, int* pitch_out) {
         ty = std::max(ty, std::max(tiles_for(c.nx, c.ny, DIR_Y, kShapesY[s]),
                                    tiles_for(c.nx, c.ny, DIR_X, kShapesX[s])));
     int npart = std::max(ty, kInitBlocks);
-    size_t bytes = 4 * sizeof(float) * nv * plane  // hi/lo x 2 buffers
+    size_t bytes = 4 * sizeof(float) * nv * plane  // value/compensation x 2 buffers
                    + 256 + sizeof(DevState) + 4 * sizeof(double) * npart + 4096;
     if (plane_out) *plane_out = plane;
     if (pitch_out) *pitch_out = pitch;
@@ -447,10 +465,11 @@ int cfd_batch_add(cfd_batch* b, const cfd_config* cfg, const double* host_ic, in
     };
     Inst& I = m.inst;
     memset(&I, 0, sizeof I);
-    for (int k = 0; k < 2; ++k) {
-        I.hi[k] = reinterpret_cast<float*>(take(sizeof(float) * nv * plane));
-        I.lo[k] = reinterpret_cast<float*>(take(sizeof(float) * nv * plane));
-    }
+    for (int k = 0; k < 2; ++k)
+        for (int w = 0; w < 2; ++w) {
+            I.q4[k][w] = reinterpret_cast<float4*>(take(sizeof(float4) * plane));
+            I.q2[k][w] = nv == 6 ? reinterpret_cast<float2*>(take(sizeof(float2) * plane)) : nullptr;
+        }
     I.st = reinterpret_cast<DevState*>(take(sizeof(DevState)));
     int npart = (int)((bytes - 4 * sizeof(float) * nv * plane - 256 - sizeof(DevState) - 4096) /
                       (4 * sizeof(double)));
@@ -511,9 +530,7 @@ int cfd_batch_add(cfd_batch* b, const cfd_config* cfg, const double* host_ic, in
             r = cfd_fail(CFD_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
             break;
         }
-        ghosted_to_mixed<<<148 * 4, 256, 0, b->stream>>>(staging, I.hi[0], I.lo[0],
-                                                         staging + ghosted, c.nx, c.ny, g, nv,
-                                                         pitch, (long long)plane);
+        ghosted_to_mixed<<<148 * 4, 256, 0, b->stream>>>(staging, I, staging + ghosted, g);
         if (c.model == CFD_MODEL_EULER)
             init_reduce<MODEL_EULER><<<kInitBlocks, 256, 0, b->stream>>>(
                 staging + ghosted, (long long)plane, pitch, c.nx, c.ny, I.eos, I.st, I.partials);
@@ -739,16 +756,10 @@ int cfd_batch_download(cfd_batch* b, int id, double* host, int layout) {
     double* tmp = nullptr;
     BTRY(cudaMalloc(&tmp, sizeof(double) * elems));
     int im = c.model == CFD_MODEL_EULER ? 1 : 2;
-    if (layout == CFD_LAYOUT_GHOSTED_AOS) {
-        mixed_to_ghosted<<<148 * 4, 256, 0, b->stream>>>(
-            m->inst.hi[cur], m->inst.lo[cur], tmp, c.nx, c.ny, g, nv, m->inst.pitch,
-            m->inst.plane, c.bc[0], c.bc[1], c.bc[2], c.bc[3], im, im + 1);
-    } else {
-        // SoA interior: reuse the ghosted kernel with g = 0 and no boundary
-        mixed_to_ghosted<<<148 * 4, 256, 0, b->stream>>>(m->inst.hi[cur], m->inst.lo[cur], tmp,
-                                                         c.nx, c.ny, 0, nv, m->inst.pitch,
-                                                         m->inst.plane, 0, 0, 0, 0, -1, -1);
-    }
+    if (layout == CFD_LAYOUT_GHOSTED_AOS)
+        mixed_to_ghosted<<<148 * 4, 256, 0, b->stream>>>(m->inst, cur, tmp, g, im, im + 1, 1);
+    else  // interior only, AoS; reordered to SoA planes below
+        mixed_to_ghosted<<<148 * 4, 256, 0, b->stream>>>(m->inst, cur, tmp, 0, -1, -1, 0);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(host, tmp, sizeof(double) * elems, cudaMemcpyDeviceToHost, b->stream);

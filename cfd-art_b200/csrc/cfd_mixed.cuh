@@ -25,11 +25,15 @@
 namespace cfd {
 namespace mixed {
 
-// Per-instance descriptor (device memory, one per solve).
+// Per-instance descriptor (device memory, one per solve).  The state of a
+// cell is stored packed: components 0-3 as one float4 and, for the Allaire
+// model, components 4-5 (E, z) as one float2, each with its compensation
+// word in a parallel plane, so a cell is read and written with 2 (Euler) or
+// 4 (Allaire) vector accesses.
 struct Inst {
-    float* hi[2];   // two state buffers, nv planes each
-    float* lo[2];
-    long long plane;
+    float4* q4[2][2];   // [state buffer][0: value, 1: compensation]
+    float2* q2[2][2];   // Allaire only
+    long long plane;    // cells per plane (pitch * ny)
     int pitch, nx, ny, nv;
     int model, limiter, wavespeed, godunov, fix_dy;
     int bc[4];       // L, R, B, T
@@ -48,12 +52,10 @@ struct MixedArgs {
     Inst* insts;
     const int* tile_inst;   // instance of each tile of this launch
     const int* tile_local;  // tile index within its instance
-    int ntiles;             // tiles of this launch; CTAs loop over them (persistent)
+    int ntiles;             // tiles of this launch
+    int chunk;              // CTA c walks tiles [c * chunk, (c + 1) * chunk) (persistent)
 };
 
-// This translation unit is compiled with -prec-div=false -prec-sqrt=false:
-// single-precision division, reciprocal and square root use the hardware
-// approximations (about 1-2 ulp), ample for the FP32 face arithmetic.
 __device__ __forceinline__ float frcp(float x) { return 1.0f / x; }
 __device__ __forceinline__ float fdiv(float a, float b) { return a / b; }
 __device__ __forceinline__ float fsqrt(float x) { return sqrtf(x); }
@@ -292,12 +294,55 @@ __device__ __forceinline__ void comp_add(float& hi, float& lo, float d) {
     lo = e;
 }
 
+template <int MODEL> __device__ __forceinline__ void load_cell(const Inst& I, int buf,
+                                                               long long off, float* h, float* l) {
+    float4 a = __ldg(I.q4[buf][0] + off), b = __ldg(I.q4[buf][1] + off);
+    h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w;
+    l[0] = b.x; l[1] = b.y; l[2] = b.z; l[3] = b.w;
+    if constexpr (MODEL == MODEL_ALLAIRE) {
+        float2 c = __ldg(I.q2[buf][0] + off), d = __ldg(I.q2[buf][1] + off);
+        h[4] = c.x; h[5] = c.y;
+        l[4] = d.x; l[5] = d.y;
+    }
+}
+
+template <int MODEL> __device__ __forceinline__ void store_cell(const Inst& I, int buf,
+                                                                long long off, const float* h,
+                                                                const float* l) {
+    I.q4[buf][0][off] = make_float4(h[0], h[1], h[2], h[3]);
+    I.q4[buf][1][off] = make_float4(l[0], l[1], l[2], l[3]);
+    if constexpr (MODEL == MODEL_ALLAIRE) {
+        I.q2[buf][0][off] = make_float2(h[4], h[5]);
+        I.q2[buf][1][off] = make_float2(l[4], l[5]);
+    }
+}
+
+// Shared-memory vectors: one float4 (+ one float2 for Allaire) per slot.
+template <int MODEL> struct SVec {
+    float4* v4;
+    float2* v2;
+    __device__ __forceinline__ void put(int s, const float* x) const {
+        v4[s] = make_float4(x[0], x[1], x[2], x[3]);
+        if constexpr (MODEL == MODEL_ALLAIRE) v2[s] = make_float2(x[4], x[5]);
+    }
+    __device__ __forceinline__ void get(int s, float* x) const {
+        float4 a = v4[s];
+        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+        if constexpr (MODEL == MODEL_ALLAIRE) {
+            float2 b = v2[s];
+            x[4] = b.x; x[5] = b.y;
+        }
+    }
+};
+
 template <int MODEL, int DIR, int TS, int NA>
 struct MTile {
     static constexpr int NV = ModelTraits<MODEL>::NV;
     static constexpr int LA = TS + 4;
     static constexpr int NSLOT = LA * NA;
     static constexpr int ST = (DIR == DIR_X) ? 1 : NA;
+    static constexpr int VB = (MODEL == MODEL_ALLAIRE) ? 24 : 16;  // bytes of one vector
+    static_assert(NSLOT == 256, "one staged cell per thread");
     __device__ static __forceinline__ int slot(int a, int b) {
         return (DIR == DIR_X) ? b * LA + a : a * NA + b;
     }
@@ -310,65 +355,85 @@ struct MTile {
             b = i - (i / NA) * NA;
         }
     }
-    // floats: hi, lo, W (NV each), Wp, Wm (NV each), F (NV + 2); bytes: flags
-    static constexpr int SMEM = (6 * NV + 2) * NSLOT * 4 + NSLOT + 64;
+    // vectors per slot: value, compensation, W, W+, W-, flux; u*, z*; flags
+    static constexpr int SMEM = 6 * VB * NSLOT + 8 * NSLOT + NSLOT + 64;
 };
 
+// Where a tile lies and whether it is skipped.
+struct TileGeom {
+    int inst, ltile, a_org, b_org, len, wid, cur;
+    bool skip;
+};
+
+template <int DIR, int TS, int NA>
+__device__ __forceinline__ TileGeom tile_geom(const MixedArgs& A, int tile) {
+    TileGeom g;
+    g.inst = A.tile_inst[tile];
+    g.ltile = A.tile_local[tile];
+    const Inst& I = A.insts[g.inst];
+    const DevState* st = I.st;
+    g.skip = !I.active || st->done || st->n >= I.max_steps;
+    g.cur = st->cur;
+    g.len = (DIR == DIR_X) ? I.nx : I.ny;
+    g.wid = (DIR == DIR_X) ? I.ny : I.nx;
+    int tiles_along = (g.len + TS - 1) / TS;
+    g.a_org = (g.ltile % tiles_along) * TS - 2;
+    g.b_org = (g.ltile / tiles_along) * NA;
+    return g;
+}
+
+// This thread's staged cell of a tile (with the boundary mirror): loads it
+// into registers; `neg` says whether the normal momentum must be negated.
 template <int MODEL, int DIR, int TS, int NA>
-__device__ __forceinline__ void mixed_tile(const MixedArgs& A, int tile, float* fsm) {
+__device__ __forceinline__ void tile_fetch(const MixedArgs& A, const TileGeom& g, float* h,
+                                           float* l, bool& neg) {
+    using Tl = MTile<MODEL, DIR, TS, NA>;
+    const Inst& I = A.insts[g.inst];
+    int a, b;
+    Tl::item(threadIdx.x, 0, Tl::LA, a, b);
+    int ga = g.a_org + a, gb = g.b_org + b;
+    int src = ga;
+    neg = false;
+    int bc_lo = (DIR == DIR_X) ? I.bc[0] : I.bc[2];
+    int bc_hi = (DIR == DIR_X) ? I.bc[1] : I.bc[3];
+    if (ga < 0) { src = -ga - 1; neg = bc_lo; }
+    else if (ga >= g.len) { src = 2 * g.len - 1 - ga; neg = bc_hi; }
+    src = min(max(src, 0), g.len - 1);
+    int gbs = min(gb, g.wid - 1);
+    long long off = (DIR == DIR_X) ? (long long)gbs * I.pitch + src : (long long)src * I.pitch + gbs;
+    load_cell<MODEL>(I, g.cur ^ (DIR == DIR_Y), off, h, l);
+}
+
+template <int MODEL, int DIR, int TS, int NA>
+__device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g, float* h,
+                                           float* l, bool& neg, int next_tile, char* smem,
+                                           double* racc) {
     using Tl = MTile<MODEL, DIR, TS, NA>;
     using MT = ModelTraits<MODEL>;
-    constexpr int NV = MT::NV, LA = Tl::LA, NSLOT = Tl::NSLOT, ST = Tl::ST, NT = 256;
-    float* sHi = fsm;
-    float* sLo = sHi + NV * NSLOT;
-    float* sW = sLo + NV * NSLOT;
-    float* sWp = sW + NV * NSLOT;
-    float* sWm = sWp + NV * NSLOT;
-    float* sF = sWm + NV * NSLOT;  // NV + 2 planes
-    unsigned char* sFl = reinterpret_cast<unsigned char*>(sF + (NV + 2) * NSLOT);
-
-    const int inst = A.tile_inst[tile];
-    const int ltile = A.tile_local[tile];
-    const Inst& I = A.insts[inst];
-    DevState* st = I.st;
-    if (!I.active || st->done || st->n >= I.max_steps) return;
-    const int cur = st->cur;
-    const float* __restrict__ ghi = I.hi[cur ^ (DIR == DIR_Y)];
-    const float* __restrict__ glo = I.lo[cur ^ (DIR == DIR_Y)];
-    float* __restrict__ ohi = I.hi[cur ^ (DIR == DIR_X)];
-    float* __restrict__ olo = I.lo[cur ^ (DIR == DIR_X)];
-    const double dt = st->dt;
-    const int len = (DIR == DIR_X) ? I.nx : I.ny;
-    const int wid = (DIR == DIR_X) ? I.ny : I.nx;
-    const int tiles_along = (len + TS - 1) / TS;
-    const int a_org = (ltile % tiles_along) * TS - 2;
-    const int b_org = (ltile / tiles_along) * NA;
-    const int bc_lo = (DIR == DIR_X) ? I.bc[0] : I.bc[2];
-    const int bc_hi = (DIR == DIR_X) ? I.bc[1] : I.bc[3];
+    constexpr int NV = MT::NV, LA = Tl::LA, NSLOT = Tl::NSLOT, ST = Tl::ST;
     const int tid = threadIdx.x;
+    auto vec = [&](int k) {
+        SVec<MODEL> v;
+        v.v4 = reinterpret_cast<float4*>(smem + k * Tl::VB * NSLOT);
+        v.v2 = reinterpret_cast<float2*>(smem + k * Tl::VB * NSLOT + 16 * NSLOT);
+        return v;
+    };
+    const SVec<MODEL> sH = vec(0), sL = vec(1), sW = vec(2), sP = vec(3), sM = vec(4), sF = vec(5);
+    float2* sUZ = reinterpret_cast<float2*>(smem + 6 * Tl::VB * NSLOT);
+    unsigned char* sFl = reinterpret_cast<unsigned char*>(smem + 6 * Tl::VB * NSLOT + 8 * NSLOT);
+
+    const Inst& I = A.insts[g.inst];
+    DevState* st = I.st;
+    const double dt = st->dt;
     const double h_flux = (DIR == DIR_X) ? I.dx : (I.fix_dy ? I.dy : I.dx);
     const double h_upd = (DIR == DIR_X) ? I.dx : I.dy;
     const float s_half = (float)(0.5 * (dt / h_flux));
     const float k_upd = (float)(dt / h_upd);
 
-    // ---- P1: load hi/lo with the boundary fill, rotate, convert --------
-    for (int i = tid; i < NSLOT; i += NT) {
+    // ---- P1: boundary sign, rotation, conversion of the fetched cell -------
+    {
         int a, b;
-        Tl::item(i, 0, LA, a, b);
-        int ga = a_org + a, gb = b_org + b;
-        int src = ga;
-        bool neg = false;
-        if (ga < 0) { src = -ga - 1; neg = bc_lo; }
-        else if (ga >= len) { src = 2 * len - 1 - ga; neg = bc_hi; }
-        src = min(max(src, 0), len - 1);
-        int gbs = min(gb, wid - 1);
-        long long off = (DIR == DIR_X) ? (long long)gbs * I.pitch + src : (long long)src * I.pitch + gbs;
-        float h[NV], l[NV];
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            h[k] = __ldg(ghi + k * I.plane + off);
-            l[k] = __ldg(glo + k * I.plane + off);
-        }
+        Tl::item(tid, 0, LA, a, b);
         if (DIR == DIR_X) {
             if (neg) { h[MT::IM] = -h[MT::IM]; l[MT::IM] = -l[MT::IM]; }
         } else {
@@ -380,54 +445,52 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, int tile, float* 
         int s = Tl::slot(a, b);
         float W[NV];
         c2p_mixed<MODEL>(I, h, l, W);
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            sHi[k * NSLOT + s] = h[k];
-            sLo[k * NSLOT + s] = l[k];
-            sW[k * NSLOT + s] = W[k];
-        }
+        sH.put(s, h);
+        sL.put(s, l);
+        sW.put(s, W);
+    }
+    // the registers are free: start loading this thread's cell of the next tile
+    if (next_tile < A.ntiles) {
+        TileGeom gn = tile_geom<DIR, TS, NA>(A, next_tile);
+        if (!gn.skip) tile_fetch<MODEL, DIR, TS, NA>(A, gn, h, l, neg);
     }
     __syncthreads();
 
     // ---- P2: slopes and evolved face states (primitive) ----------------
-    if (!I.godunov) {
-        for (int i = tid; i < (LA - 2) * NA; i += NT) {
-            int a, b;
-            Tl::item(i, 1, LA - 2, a, b);
-            int s = Tl::slot(a, b);
-            float W[NV], d[NV], X[NV], Wt[NV];
+    if (!I.godunov && tid < (LA - 2) * NA) {
+        int a, b;
+        Tl::item(tid, 1, LA - 2, a, b);
+        int s = Tl::slot(a, b);
+        float W[NV], Wl[NV], Wr[NV], d[NV], X[NV], Wt[NV];
+        sW.get(s, W);
+        sW.get(s - ST, Wl);
+        sW.get(s + ST, Wr);
 #pragma unroll
-            for (int k = 0; k < NV; ++k) {
-                W[k] = sW[k * NSLOT + s];
-                d[k] = limit_f(I.limiter, W[k] - sW[k * NSLOT + s - ST], sW[k * NSLOT + s + ST] - W[k]);
-            }
-            unsigned fl = 0;
+        for (int k = 0; k < NV; ++k) d[k] = limit_f(I.limiter, W[k] - Wl[k], Wr[k] - W[k]);
+        unsigned fl = 0;
 #pragma unroll
-            for (int k = 0; k < NV; ++k) Wt[k] = W[k] + 0.5f * d[k];
-            if (phys_prim<MODEL>(I, Wt)) fl |= 1u;
+        for (int k = 0; k < NV; ++k) Wt[k] = W[k] + 0.5f * d[k];
+        if (phys_prim<MODEL>(I, Wt)) fl |= 1u;
 #pragma unroll
-            for (int k = 0; k < NV; ++k) Wt[k] = W[k] - 0.5f * d[k];
-            if (phys_prim<MODEL>(I, Wt)) fl |= 2u;
-            jac_f<MODEL>(I, W, d, s_half, X);
+        for (int k = 0; k < NV; ++k) Wt[k] = W[k] - 0.5f * d[k];
+        if (phys_prim<MODEL>(I, Wt)) fl |= 2u;
+        jac_f<MODEL>(I, W, d, s_half, X);
 #pragma unroll
-            for (int k = 0; k < NV; ++k) Wt[k] = (W[k] + 0.5f * d[k]) - X[k];
-            if (phys_prim<MODEL>(I, Wt)) fl |= 4u;
+        for (int k = 0; k < NV; ++k) Wt[k] = (W[k] + 0.5f * d[k]) - X[k];
+        if (phys_prim<MODEL>(I, Wt)) fl |= 4u;
+        sP.put(s, Wt);
 #pragma unroll
-            for (int k = 0; k < NV; ++k) sWp[k * NSLOT + s] = Wt[k];
-#pragma unroll
-            for (int k = 0; k < NV; ++k) Wt[k] = (W[k] - 0.5f * d[k]) - X[k];
-            if (phys_prim<MODEL>(I, Wt)) fl |= 8u;
-#pragma unroll
-            for (int k = 0; k < NV; ++k) sWm[k * NSLOT + s] = Wt[k];
-            sFl[s] = (unsigned char)fl;
-        }
+        for (int k = 0; k < NV; ++k) Wt[k] = (W[k] - 0.5f * d[k]) - X[k];
+        if (phys_prim<MODEL>(I, Wt)) fl |= 8u;
+        sM.put(s, Wt);
+        sFl[s] = (unsigned char)fl;
     }
     __syncthreads();
 
     // ---- P3: HLLC per face -------------------------------------------------
-    for (int i = tid; i < (TS + 1) * NA; i += NT) {
+    if (tid < (TS + 1) * NA) {
         int a, b;
-        Tl::item(i, 2, TS + 1, a, b);
+        Tl::item(tid, 2, TS + 1, a, b);
         int sR = Tl::slot(a, b), sL = sR - ST;
         float WL[NV], WR[NV];
         bool first = true;
@@ -437,166 +500,201 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, int tile, float* 
             // fallback uses the cell states too
             if ((fL & 1u) && (fR & 2u) && (fL & 4u) && (fR & 8u)) {
                 first = false;
-#pragma unroll
-                for (int k = 0; k < NV; ++k) {
-                    WL[k] = sWp[k * NSLOT + sL];
-                    WR[k] = sWm[k * NSLOT + sR];
-                }
+                sP.get(sL, WL);
+                sM.get(sR, WR);
             }
         }
         if (first) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) {
-                WL[k] = sW[k * NSLOT + sL];
-                WR[k] = sW[k * NSLOT + sR];
-            }
+            sW.get(sL, WL);
+            sW.get(sR, WR);
         }
         float F[NV + 2];
         hllc_prim<MODEL>(I, WL, WR, F);
-#pragma unroll
-        for (int k = 0; k < NV + 2; ++k) sF[k * NSLOT + sR] = F[k];
+        sF.put(sR, F);
+        sUZ[sR] = make_float2(F[NV], MODEL == MODEL_ALLAIRE ? F[NV + 1] : 0.0f);
     }
     __syncthreads();
 
     // ---- P4: compensated update, store, reduce -----------------------------
     double r_mu = 0.0, r_mv = 0.0, r_m1 = 0.0, r_m2 = 0.0;
-    for (int i = tid; i < TS * NA; i += NT) {
+    if (tid < TS * NA) {
         int a, b;
-        Tl::item(i, 2, TS, a, b);
-        int ga = a_org + a, gb = b_org + b;
-        if (ga >= len || gb >= wid) continue;
-        int s = Tl::slot(a, b);
-        float h[NV], l[NV];
+        Tl::item(tid, 2, TS, a, b);
+        int ga = g.a_org + a, gb = g.b_org + b;
+        if (ga < g.len && gb < g.wid) {
+            int s = Tl::slot(a, b);
+            float hh[NV], ll[NV], FL[NV], FR[NV];
+            sH.get(s, hh);
+            sL.get(s, ll);
+            sF.get(s, FL);
+            sF.get(s + ST, FR);
+            float oh[NV], ol[NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            h[k] = sHi[k * NSLOT + s];
-            l[k] = sLo[k * NSLOT + s];
-        }
-        float oh[NV], ol[NV];
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            oh[k] = h[k];
-            ol[k] = l[k];
-        }
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            if (MODEL == MODEL_ALLAIRE && k == 5) continue;
-            float dlt = k_upd * (sF[k * NSLOT + s] - sF[k * NSLOT + s + ST]);
-            comp_add(h[k], l[k], dlt);
-        }
-        if constexpr (MODEL == MODEL_ALLAIRE) {
-            float usL = sF[NV * NSLOT + s], usR = sF[NV * NSLOT + s + ST];
-            float zsL = sF[(NV + 1) * NSLOT + s], zsR = sF[(NV + 1) * NSLOT + s + ST];
-            float z = h[5];
-            float dz;
-            if (I.godunov) {
-                float zL = sHi[5 * NSLOT + s - ST], zR = sHi[5 * NSLOT + s + ST];
-                dz = -k_upd * ((zR - z) * fminf_s(0.0f, usR) + (z - zL) * fmaxf_s(0.0f, usL));
-            } else {
-                dz = -k_upd * ((usR * zsR - usL * zsL) - z * (usR - usL));
+            for (int k = 0; k < NV; ++k) {
+                oh[k] = hh[k];
+                ol[k] = ll[k];
             }
-            comp_add(h[5], l[5], dz);
-            float zlo = (float)I.z_min, zhi = (float)(1.0 - I.z_min);
-            if (h[5] + l[5] < zlo) { h[5] = zlo; l[5] = (float)(I.z_min - (double)zlo); }
-            if (h[5] + l[5] > zhi) { h[5] = zhi; l[5] = (float)((1.0 - I.z_min) - (double)zhi); }
-            if (h[0] < 0.0f) { h[0] = 0.0f; l[0] = 0.0f; }
-            if (h[1] < 0.0f) { h[1] = 0.0f; l[1] = 0.0f; }
-        }
-        if (DIR == DIR_Y) {  // rotate back
-            float t = h[MT::IM], tl = l[MT::IM];
-            h[MT::IM] = -h[MT::IT]; l[MT::IM] = -l[MT::IT];
-            h[MT::IT] = t; l[MT::IT] = tl;
-            float t2 = oh[MT::IM], t2l = ol[MT::IM];
-            oh[MT::IM] = -oh[MT::IT]; ol[MT::IM] = -ol[MT::IT];
-            oh[MT::IT] = t2; ol[MT::IT] = t2l;
-        }
-        float Wn[NV];
-        c2p_mixed<MODEL>(I, h, l, Wn);
-        if constexpr (MODEL == MODEL_EULER) {
-            // density / energy restore as in the plain form (rare)
-            if (!(h[0] > 1e-12f) || !(Wn[3] + I.gp1f > 0.0f)) {
-                float Wo[NV];
-                c2p_mixed<MODEL>(I, oh, ol, Wo);
-                float rho = h[0] > 1e-12f ? h[0] : oh[0];
-                float u = Wn[1], v = Wn[2];
-                float p = (Wn[3] + I.gp1f > 0.0f) ? Wn[3] : Wo[3];
-                h[0] = rho; l[0] = 0.f;
-                h[1] = rho * u; l[1] = 0.f;
-                h[2] = rho * v; l[2] = 0.f;
-                h[3] = fdiv(p + I.gp1f, I.gm1_1f) + 0.5f * rho * (u * u + v * v); l[3] = 0.f;
-                Wn[0] = rho;
-                Wn[3] = p;
-            }
-        }
-        long long off = (DIR == DIR_X) ? (long long)gb * I.pitch + ga : (long long)ga * I.pitch + gb;
 #pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            ohi[k * I.plane + off] = h[k];
-            olo[k * I.plane + off] = l[k];
-        }
-        if (DIR == DIR_Y) {
-            float c = sound_f<MODEL>(I, Wn);
-            float u = Wn[MT::IM], v = Wn[MT::IT];
-            r_mu = smax(r_mu, (double)(fabsf(u) + c));
-            r_mv = smax(r_mv, (double)(fabsf(v) + c));
+            for (int k = 0; k < NV; ++k) {
+                if (MODEL == MODEL_ALLAIRE && k == 5) continue;
+                comp_add(hh[k], ll[k], k_upd * (FL[k] - FR[k]));
+            }
+            if constexpr (MODEL == MODEL_ALLAIRE) {
+                float2 uzL = sUZ[s], uzR = sUZ[s + ST];
+                float usL = uzL.x, usR = uzR.x, zsL = uzL.y, zsR = uzR.y;
+                float z = hh[5];
+                float dz;
+                if (I.godunov) {
+                    float zL = sH.v2[s - ST].y, zR = sH.v2[s + ST].y;
+                    dz = -k_upd * ((zR - z) * fminf_s(0.0f, usR) + (z - zL) * fmaxf_s(0.0f, usL));
+                } else {
+                    dz = -k_upd * ((usR * zsR - usL * zsL) - z * (usR - usL));
+                }
+                comp_add(hh[5], ll[5], dz);
+                float zlo = (float)I.z_min, zhi = (float)(1.0 - I.z_min);
+                if (hh[5] + ll[5] < zlo) { hh[5] = zlo; ll[5] = (float)(I.z_min - (double)zlo); }
+                if (hh[5] + ll[5] > zhi) { hh[5] = zhi; ll[5] = (float)((1.0 - I.z_min) - (double)zhi); }
+                if (hh[0] < 0.0f) { hh[0] = 0.0f; ll[0] = 0.0f; }
+                if (hh[1] < 0.0f) { hh[1] = 0.0f; ll[1] = 0.0f; }
+            }
+            if (DIR == DIR_Y) {  // rotate back
+                float t = hh[MT::IM], tl = ll[MT::IM];
+                hh[MT::IM] = -hh[MT::IT]; ll[MT::IM] = -ll[MT::IT];
+                hh[MT::IT] = t; ll[MT::IT] = tl;
+                float t2 = oh[MT::IM], t2l = ol[MT::IM];
+                oh[MT::IM] = -oh[MT::IT]; ol[MT::IM] = -ol[MT::IT];
+                oh[MT::IT] = t2; ol[MT::IT] = t2l;
+            }
+            float Wn[NV];
+            c2p_mixed<MODEL>(I, hh, ll, Wn);
             if constexpr (MODEL == MODEL_EULER) {
-                r_m1 += (double)h[0] + (double)l[0];
-            } else {
-                r_m1 += (double)h[0] + (double)l[0];
-                r_m2 += (double)h[1] + (double)l[1];
+                // density / energy restore as in the plain form (rare)
+                if (!(hh[0] > 1e-12f) || !(Wn[3] + I.gp1f > 0.0f)) {
+                    float Wo[NV];
+                    c2p_mixed<MODEL>(I, oh, ol, Wo);
+                    float rho = hh[0] > 1e-12f ? hh[0] : oh[0];
+                    float u = Wn[1], v = Wn[2];
+                    float p = (Wn[3] + I.gp1f > 0.0f) ? Wn[3] : Wo[3];
+                    hh[0] = rho; ll[0] = 0.f;
+                    hh[1] = rho * u; ll[1] = 0.f;
+                    hh[2] = rho * v; ll[2] = 0.f;
+                    hh[3] = fdiv(p + I.gp1f, I.gm1_1f) + 0.5f * rho * (u * u + v * v); ll[3] = 0.f;
+                    Wn[0] = rho;
+                    Wn[3] = p;
+                }
+            }
+            long long off = (DIR == DIR_X) ? (long long)gb * I.pitch + ga : (long long)ga * I.pitch + gb;
+            store_cell<MODEL>(I, g.cur ^ (DIR == DIR_X), off, hh, ll);
+            if (DIR == DIR_Y) {
+                float c = sound_f<MODEL>(I, Wn);
+                r_mu = (double)(fabsf(Wn[MT::IM]) + c);
+                r_mv = (double)(fabsf(Wn[MT::IT]) + c);
+                r_m1 = (double)hh[0] + (double)ll[0];
+                if constexpr (MODEL == MODEL_ALLAIRE) r_m2 = (double)hh[1] + (double)ll[1];
             }
         }
     }
-    if constexpr (DIR == DIR_Y) {
-
-        // ---- per-instance reduction; the instance's last CTA picks its dt ------
-        __shared__ double red[4][8];
-        __shared__ bool is_last;
-        for (int o = 16; o > 0; o >>= 1) {
-            r_mu = smax(r_mu, __shfl_down_sync(0xffffffffu, r_mu, o));
-            r_mv = smax(r_mv, __shfl_down_sync(0xffffffffu, r_mv, o));
-            r_m1 += __shfl_down_sync(0xffffffffu, r_m1, o);
-            r_m2 += __shfl_down_sync(0xffffffffu, r_m2, o);
-        }
-        if ((tid & 31) == 0) {
-            red[0][tid >> 5] = r_mu;
-            red[1][tid >> 5] = r_mv;
-            red[2][tid >> 5] = r_m1;
-            red[3][tid >> 5] = r_m2;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            double mu = red[0][0], mv = red[1][0], m1 = red[2][0], m2 = red[3][0];
-            for (int w = 1; w < NT / 32; ++w) {
-                mu = smax(mu, red[0][w]);
-                mv = smax(mv, red[1][w]);
-                m1 += red[2][w];
-                m2 += red[3][w];
-            }
-            double* p = I.partials + 4 * ltile;
-            p[0] = mu;
-            p[1] = mv;
-            p[2] = m1;
-            p[3] = m2;
-            __threadfence();
-            unsigned t = atomicAdd(&st->ticket, 1u);
-            is_last = (t == (unsigned)I.tiles_y - 1);
-        }
-        __syncthreads();
-        if (is_last) {
-            __threadfence();
-            finish_reduction(st, I.partials, I.tiles_y, 1, dt, 0);
-        }
+    if constexpr (DIR == DIR_Y) {  // this thread's wave speeds and masses
+        racc[0] = smax(racc[0], r_mu);
+        racc[1] = smax(racc[1], r_mv);
+        racc[2] += r_m1;
+        racc[3] += r_m2;
     }
 }
 
+// End of the run of an instance's tiles processed by this CTA (y sweep):
+// block-reduce the run's wave speeds and masses into the instance's partial
+// slot, count the run's tiles, and let the CTA that completes the count pick
+// the instance's dt.  CTA c walks the contiguous tile range
+// [c * chunk, (c + 1) * chunk), so it meets an instance (tiles [t0, t0 + n))
+// in at most one run, and the CTAs that do are c0 = t0 / chunk ..
+// (t0 + n - 1) / chunk: slot c - c0 is written exactly once per sweep.
+__device__ __forceinline__ void flush_run(const MixedArgs& A, int inst, int slot, int nslots,
+                                          int count, double* racc, double dt) {
+    const Inst& I = A.insts[inst];
+    DevState* st = I.st;
+    __shared__ double red[4][8];
+    __shared__ bool is_last;
+    const int tid = threadIdx.x;
+    double mu = racc[0], mv = racc[1], m1 = racc[2], m2 = racc[3];
+    for (int o = 16; o > 0; o >>= 1) {
+        mu = smax(mu, __shfl_down_sync(0xffffffffu, mu, o));
+        mv = smax(mv, __shfl_down_sync(0xffffffffu, mv, o));
+        m1 += __shfl_down_sync(0xffffffffu, m1, o);
+        m2 += __shfl_down_sync(0xffffffffu, m2, o);
+    }
+    if ((tid & 31) == 0) {
+        red[0][tid >> 5] = mu;
+        red[1][tid >> 5] = mv;
+        red[2][tid >> 5] = m1;
+        red[3][tid >> 5] = m2;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mu = red[0][0], mv = red[1][0], m1 = red[2][0], m2 = red[3][0];
+        for (int w = 1; w < 8; ++w) {
+            mu = smax(mu, red[0][w]);
+            mv = smax(mv, red[1][w]);
+            m1 += red[2][w];
+            m2 += red[3][w];
+        }
+        double* p = I.partials + 4 * slot;
+        p[0] = mu;
+        p[1] = mv;
+        p[2] = m1;
+        p[3] = m2;
+        __threadfence();
+        unsigned t = atomicAdd(&st->ticket, (unsigned)count);
+        is_last = (t + (unsigned)count == (unsigned)I.tiles_y);
+    }
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        finish_reduction(st, I.partials, nslots, 1, dt, 0);
+    }
+    racc[0] = racc[1] = racc[2] = racc[3] = 0.0;
+}
+
 // Persistent sweep: a fixed grid of CTAs walks the tile list of every
-// instance in the launch.
+// instance in the launch; each thread loads its cell of the next tile while
+// the current tile is being computed.
 template <int MODEL, int DIR, int TS, int NA>
-__global__ void __launch_bounds__(256) mixed_sweep_kernel(MixedArgs A) {
-    extern __shared__ __align__(16) float fsm[];
-    for (int tile = blockIdx.x; tile < A.ntiles; tile += gridDim.x) {
-        mixed_tile<MODEL, DIR, TS, NA>(A, tile, fsm);
+__global__ void __launch_bounds__(256, MODEL == MODEL_EULER ? 4 : 3) mixed_sweep_kernel(MixedArgs A) {
+    extern __shared__ __align__(16) char msm[];
+    constexpr int NV = ModelTraits<MODEL>::NV;
+    float h[NV], l[NV];
+    bool neg = false;
+    const int t_begin = blockIdx.x * A.chunk;
+    const int t_end = min(t_begin + A.chunk, A.ntiles);
+    if (t_begin >= t_end) return;
+    TileGeom g = tile_geom<DIR, TS, NA>(A, t_begin);
+    if (!g.skip) tile_fetch<MODEL, DIR, TS, NA>(A, g, h, l, neg);
+    double racc[4] = {0.0, 0.0, 0.0, 0.0};
+    int run_first = t_begin, run_count = 0;
+    for (int tile = t_begin; tile < t_end; ++tile) {
+        int next = tile + 1 < t_end ? tile + 1 : A.ntiles;  // A.ntiles: none
+        const int inst = g.inst;
+        const bool skip = g.skip;
+        const double dt = skip ? 0.0 : A.insts[inst].st->dt;
+        if (!skip) {
+            mixed_tile<MODEL, DIR, TS, NA>(A, g, h, l, neg, next, msm, racc);
+            ++run_count;
+        } else if (next < A.ntiles) {
+            TileGeom gn = tile_geom<DIR, TS, NA>(A, next);
+            if (!gn.skip) tile_fetch<MODEL, DIR, TS, NA>(A, gn, h, l, neg);
+        }
+        bool run_ends = next >= A.ntiles || A.tile_inst[next] != inst;
+        if (DIR == DIR_Y && run_ends && run_count > 0) {
+            int t0 = run_first - A.tile_local[run_first];  // first tile of the instance
+            int c0 = t0 / A.chunk;
+            int nslots = (t0 + A.insts[inst].tiles_y - 1) / A.chunk - c0 + 1;
+            flush_run(A, inst, (int)blockIdx.x - c0, nslots, run_count, racc, dt);
+        }
+        if (run_ends) {
+            run_count = 0;
+            run_first = next;
+        }
+        if (next < A.ntiles) g = tile_geom<DIR, TS, NA>(A, next);
         __syncthreads();  // shared memory is reused by the next tile
     }
 }

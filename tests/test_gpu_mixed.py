@@ -77,6 +77,19 @@ def test_mixed_reference_cases(case, nx, ny):
     assert l1 <= TOL_MIXED_L1
 
 
+@pytest.mark.parametrize("case,nx,ny", [("circular_explosion", 160, 140), ("totem_pole_1", 150, 170)])
+def test_mixed_reflective_walls(case, nx, ny):
+    """Wall-dominated Euler cases (reflective sides hit by blast waves): the
+    reflective ghost sign must follow each tile's own boundary cells."""
+    cfg = G.case_config(G.EULER, case, nx, ny)
+    ic = G.case_ic(cfg, case)
+    ref, _ = _fp64_run(cfg, ic, 250)
+    out, _ = _mixed_run(cfg, ic, 250)
+    l1, linf = _errors(out, ref, "euler")
+    print(f"{case}: mixed vs FP64 L1 {l1:.2e} Linf {linf:.2e}")
+    assert l1 <= TOL_MIXED_L1
+
+
 def _members():
     out = []
     for k, (rec, nx, ny) in enumerate([("shock_bubbles", 96, 200), ("shock_bubbles", 300, 64),

@@ -65,15 +65,15 @@ def test_mixed_served_close_to_fp64_served():
 
 
 def test_late_arrivals_join_running_work_and_budget_holds():
-    cfg = G.recipe_config("shock_bubbles", 384, 384)
+    cfg = G.recipe_config("shock_bubbles", 1024, 1024)
     ic = G.recipe_ic(cfg, "shock_bubbles", nbubbles=8)
     need = G.Batch.member_bytes(cfg)
     with G.Server(G.MIXED, budget_bytes=int(need * 2.5), ticks_per_round=4) as srv:
-        first = srv.submit(cfg, ic, 400)
+        first = srv.submit(cfg, ic, 6000)  # ~0.6 s of work
         time.sleep(0.05)
-        late = [srv.submit(cfg, ic, 40) for _ in range(4)]  # at most 2 resident at a time
+        late = [srv.submit(cfg, ic, 20) for _ in range(4)]  # at most 2 resident at a time
         peak = 0
-        for _ in range(200):
+        for _ in range(2000):
             st = srv.stats()
             peak = max(peak, st.running)
             assert st.used_bytes <= st.budget_bytes
