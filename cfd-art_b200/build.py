@@ -31,6 +31,7 @@ INC = [f"-I{ROOT / 'include'}", f"-I{PKG / 'csrc'}"]
 CUDA_SOURCES = [
     ("csrc/cfd_api.cu", ["--fmad=false"]),
     ("csrc/cfd_noalloc.cu", ["--fmad=false"]),
+    ("csrc/cfd_ic.cu", ["--fmad=false"]),
     # mixed precision: FP32 with contraction and flush-to-zero
     ("csrc/cfd_batch.cu", ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
 ]

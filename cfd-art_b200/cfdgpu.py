@@ -119,6 +119,8 @@ def lib() -> C.CDLL:
             "cfd_destroy": (ip, [vp]),
             "cfd_upload": (ip, [vp, dp, ip, ip, C.c_double]),
             "cfd_upload_device": (ip, [vp, vp, ip, C.c_double]),
+            "cfd_upload_recipe": (ip, [vp, ip, C.c_uint64, ip, ip, C.c_double]),
+            "cfd_upload_case": (ip, [vp, C.c_char_p, C.c_uint64, ip, C.c_double]),
             "cfd_download": (ip, [vp, dp, ip]),
             "cfd_compute_dt": (ip, [vp, ip, C.c_double, dp]),
             "cfd_step": (ip, [vp, C.c_double]),
@@ -143,6 +145,7 @@ def lib() -> C.CDLL:
             "cfd_batch_destroy": (ip, [vp]),
             "cfd_batch_member_bytes": (ip, [cfgp, C.POINTER(C.c_size_t)]),
             "cfd_batch_add": (ip, [vp, cfgp, dp, ip, C.POINTER(ip)]),
+            "cfd_batch_add_recipe": (ip, [vp, cfgp, ip, C.c_uint64, ip, ip, C.POINTER(ip)]),
             "cfd_batch_remove": (ip, [vp, ip]),
             "cfd_batch_size": (ip, [vp, C.POINTER(ip), C.POINTER(C.c_size_t),
                                     C.POINTER(C.c_size_t)]),
@@ -157,6 +160,8 @@ def lib() -> C.CDLL:
             "cfd_batch_download": (ip, [vp, ip, dp, ip]),
             "cfd_server_create": (ip, [C.POINTER(ServerOptions), C.POINTER(vp)]),
             "cfd_server_submit": (ip, [vp, cfgp, dp, ip, C.POINTER(C.c_int64)]),
+            "cfd_server_submit_recipe": (ip, [vp, cfgp, ip, C.c_uint64, ip, ip,
+                                              C.POINTER(C.c_int64)]),
             "cfd_server_wait": (ip, [vp, C.c_int64, C.c_double, C.POINTER(RequestInfo), dp]),
             "cfd_server_release": (ip, [vp, C.c_int64]),
             "cfd_server_get_stats": (ip, [vp, C.POINTER(ServerStats)]),
@@ -258,6 +263,17 @@ class Solver:
 
     def upload_device(self, ptr: int, n: int = 0, t: float = 0.0):
         check(lib().cfd_upload_device(self._h, C.c_void_p(ptr), n, t), "cfd_upload_device")
+
+    def upload_recipe(self, name: str, seed: int = 20261203, nbubbles: int = 32, n: int = 0,
+                      t: float = 0.0):
+        """Builds a recipe's initial condition on the device."""
+        check(lib().cfd_upload_recipe(self._h, RECIPE[name], seed, nbubbles, n, t),
+              f"cfd_upload_recipe({name})")
+
+    def upload_case(self, test_case: str, seed: int = 0, n: int = 0, t: float = 0.0):
+        """Builds a named test case's initial condition on the device."""
+        check(lib().cfd_upload_case(self._h, test_case.encode(), seed, n, t),
+              f"cfd_upload_case({test_case})")
 
     def download(self, layout: int = GHOSTED_AOS, out: np.ndarray | None = None) -> np.ndarray:
         c = self.cfg
@@ -366,6 +382,15 @@ class Batch:
         self.cfgs[i.value] = cfg.copy()
         return i.value
 
+    def add_recipe(self, cfg: Config, name: str, seed: int = 20261203, nbubbles: int = 32,
+                   max_steps: int = 0) -> int:
+        """Adds a member whose initial condition is built on the device."""
+        i = C.c_int()
+        check(lib().cfd_batch_add_recipe(self._h, C.byref(cfg), RECIPE[name], seed, nbubbles,
+                                         max_steps, C.byref(i)), "cfd_batch_add_recipe")
+        self.cfgs[i.value] = cfg.copy()
+        return i.value
+
     def try_add(self, cfg: Config, grid: np.ndarray, max_steps: int = 0) -> int | None:
         """Like add, but returns None when the member does not fit the budget."""
         i = C.c_int()
@@ -468,6 +493,14 @@ class Server:
         rid = C.c_int64()
         check(lib().cfd_server_submit(self._h, C.byref(cfg), _dp(np.ascontiguousarray(grid)),
                                       steps, C.byref(rid)), "cfd_server_submit")
+        self.cfgs[rid.value] = cfg.copy()
+        return rid.value
+
+    def submit_recipe(self, cfg: Config, name: str, seed: int, nbubbles: int, steps: int) -> int:
+        """Queues a solve whose initial condition is built on the device."""
+        rid = C.c_int64()
+        check(lib().cfd_server_submit_recipe(self._h, C.byref(cfg), RECIPE[name], seed, nbubbles,
+                                             steps, C.byref(rid)), "cfd_server_submit_recipe")
         self.cfgs[rid.value] = cfg.copy()
         return rid.value
 

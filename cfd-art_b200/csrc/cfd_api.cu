@@ -15,7 +15,9 @@
 
 #include "../../include/cfdgpu.h"
 #include "cfd_error.h"
+#include "cfd_ic.h"
 #include "cfd_sweep.cuh"
+#include "ic_builders.h"
 
 using namespace cfd;
 
@@ -591,6 +593,41 @@ int cfd_upload_device(cfd_solver* s, const double* dev, int n, double t) {
     if ((r = enqueue_reduce(s))) return r;
     s->uploaded = true;
     return CFD_OK;
+}
+
+// Builds a shape program's state on the device in the solver's first
+// buffer, then sets the time and reduces the wave speeds as cfd_upload does.
+static int upload_program(cfd_solver* s, const std::vector<cfdic::Op>& ops, const cfdic::Eos& q,
+                          int n, double t) {
+    const cfd_config& c = s->cfg;
+    cfdic::Geom geo{c.x0, c.y0, c.dx, c.dy};
+    CUDA_TRY(cfdic::build_device(ops, q, geo, c.nx, c.ny, s->buf[0], s->plane, s->pitch,
+                                 s->stream));
+    int r;
+    if ((r = set_time(s, n, t))) return r;
+    if ((r = enqueue_reduce(s))) return r;
+    s->uploaded = true;
+    return CFD_OK;
+}
+
+int cfd_upload_recipe(cfd_solver* s, int recipe, uint64_t seed, int nbubbles, int n, double t) {
+    if (!s) return fail(CFD_ERR_INVALID, "null argument");
+    std::vector<cfdic::Op> ops;
+    cfdic::Eos q;
+    int r = cfdic::recipe_program(&s->cfg, recipe, seed, nbubbles, ops, q);
+    if (r) return fail(r, "recipe %d does not apply to this configuration", recipe);
+    return upload_program(s, ops, q, n, t);
+}
+
+int cfd_upload_case(cfd_solver* s, const char* test_case, uint64_t seed, int n, double t) {
+    if (!s || !test_case) return fail(CFD_ERR_INVALID, "null argument");
+    std::vector<cfdic::Op> ops;
+    cfdic::Eos q;
+    int r = cfdic::case_program(&s->cfg, test_case, seed, ops, q);
+    if (r == CFD_ERR_UNSUPPORTED)
+        return fail(r, "test case %s is built on the host only (cfd_case_ic)", test_case);
+    if (r) return fail(r, "unknown test case %s", test_case);
+    return upload_program(s, ops, q, n, t);
 }
 
 static int current_buffer(cfd_solver* s, int& cur) {

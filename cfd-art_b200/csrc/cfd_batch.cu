@@ -25,7 +25,9 @@
 
 #include "../../include/cfdgpu.h"
 #include "cfd_error.h"
+#include "cfd_ic.h"
 #include "cfd_mixed.cuh"
+#include "ic_builders.h"
 
 using namespace cfd;
 using namespace cfd::mixed;
@@ -113,6 +115,30 @@ __global__ void ghosted_to_mixed(const double* __restrict__ src, Inst I,
             h[k] = (float)x;
             l[k] = (float)(x - (double)h[k]);
             soa[k * I.plane + o] = x;
+        }
+        I.q4[0][0][o] = make_float4(h[0], h[1], h[2], h[3]);
+        I.q4[0][1][o] = make_float4(l[0], l[1], l[2], l[3]);
+        if (nv == 6) {
+            I.q2[0][0][o] = make_float2(h[4], h[5]);
+            I.q2[0][1][o] = make_float2(l[4], l[5]);
+        }
+    }
+}
+
+// FP64 SoA planes (the instance's pitch and plane) -> packed value /
+// compensation planes of buffer 0.
+__global__ void soa_to_mixed(const double* __restrict__ soa, Inst I) {
+    long long n = (long long)I.nx * I.ny;
+    const int nv = I.nv;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(idx / I.nx), j = (int)(idx % I.nx);
+        long long o = (long long)i * I.pitch + j;
+        float h[6], l[6];
+        for (int k = 0; k < nv; ++k) {
+            double x = soa[k * I.plane + o];
+            h[k] = (float)x;
+            l[k] = (float)(x - (double)h[k]);
         }
         I.q4[0][0][o] = make_float4(h[0], h[1], h[2], h[3]);
         I.q4[0][1][o] = make_float4(l[0], l[1], l[2], l[3]);
@@ -432,9 +458,11 @@ int cfd_batch_member_bytes(const cfd_config* cfg, size_t* bytes) {
     return CFD_OK;
 }
 
-int cfd_batch_add(cfd_batch* b, const cfd_config* cfg, const double* host_ic, int max_steps,
-                  int* id_out) {
-    if (!b || !cfg || !host_ic || !id_out) return cfd_fail(CFD_ERR_INVALID, "null argument");
+// Adds a member whose initial state is either a ghosted AoS host grid or a
+// shape program built on the device.
+static int add_member(cfd_batch* b, const cfd_config* cfg, const double* host_ic,
+                      const std::vector<cfdic::Op>* prog, const cfdic::Eos* prog_eos,
+                      int max_steps, int* id_out) {
     const cfd_config& c = *cfg;
     if (c.model != CFD_MODEL_EULER && c.model != CFD_MODEL_ALLAIRE)
         return cfd_fail(CFD_ERR_INVALID, "unknown model %d", c.model);
@@ -504,11 +532,11 @@ int cfd_batch_add(cfd_batch* b, const cfd_config* cfg, const double* host_ic, in
     I.gp1f = (float)I.eos.gp1;
     I.max_steps = max_steps;
     I.active = 1;
-    // upload: the ghosted FP64 grid goes through the second buffer pair as
-    // staging (its 2 x nv x plane floats hold the ghosted doubles when the
-    // grid is large enough; otherwise a temporary buffer is used)
+    // upload: the ghosted FP64 grid (or the device-built SoA state) goes
+    // through a temporary staging buffer, followed by the FP64 SoA copy the
+    // initial wave-speed reduction reads
     int g = c.flux_solver == CFD_FLUX_GODUNOV ? 1 : 2;
-    size_t ghosted = (size_t)nv * (c.nx + 2 * g) * (size_t)(c.ny + 2 * g);
+    size_t ghosted = host_ic ? (size_t)nv * (c.nx + 2 * g) * (size_t)(c.ny + 2 * g) : 0;
     size_t soa = (size_t)nv * plane;
     double* staging = nullptr;
     cudaError_t e = cudaMalloc(&staging, sizeof(double) * (ghosted + soa));
@@ -524,13 +552,26 @@ int cfd_batch_add(cfd_batch* b, const cfd_config* cfg, const double* host_ic, in
     init.dy = c.dy;
     int r = CFD_OK;
     do {
-        if ((e = cudaMemcpyAsync(I.st, &init, sizeof init, cudaMemcpyHostToDevice, b->stream)) ||
-            (e = cudaMemcpyAsync(staging, host_ic, sizeof(double) * ghosted, cudaMemcpyHostToDevice,
-                                 b->stream))) {
+        if ((e = cudaMemcpyAsync(I.st, &init, sizeof init, cudaMemcpyHostToDevice, b->stream))) {
             r = cfd_fail(CFD_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
             break;
         }
-        ghosted_to_mixed<<<148 * 4, 256, 0, b->stream>>>(staging, I, staging + ghosted, g);
+        if (host_ic) {
+            if ((e = cudaMemcpyAsync(staging, host_ic, sizeof(double) * ghosted,
+                                     cudaMemcpyHostToDevice, b->stream))) {
+                r = cfd_fail(CFD_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+                break;
+            }
+            ghosted_to_mixed<<<148 * 4, 256, 0, b->stream>>>(staging, I, staging + ghosted, g);
+        } else {
+            cfdic::Geom geo{c.x0, c.y0, c.dx, c.dy};
+            if ((e = cfdic::build_device(*prog, *prog_eos, geo, c.nx, c.ny, staging,
+                                         (long long)plane, pitch, b->stream))) {
+                r = cfd_fail(CFD_ERR_CUDA, "initial condition: %s", cudaGetErrorString(e));
+                break;
+            }
+            soa_to_mixed<<<148 * 4, 256, 0, b->stream>>>(staging, I);
+        }
         if (c.model == CFD_MODEL_EULER)
             init_reduce<MODEL_EULER><<<kInitBlocks, 256, 0, b->stream>>>(
                 staging + ghosted, (long long)plane, pitch, c.nx, c.ny, I.eos, I.st, I.partials);
@@ -552,6 +593,22 @@ int cfd_batch_add(cfd_batch* b, const cfd_config* cfg, const double* host_ic, in
     b->dirty = true;
     *id_out = m.id;
     return CFD_OK;
+}
+
+int cfd_batch_add(cfd_batch* b, const cfd_config* cfg, const double* host_ic, int max_steps,
+                  int* id_out) {
+    if (!b || !cfg || !host_ic || !id_out) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    return add_member(b, cfg, host_ic, nullptr, nullptr, max_steps, id_out);
+}
+
+int cfd_batch_add_recipe(cfd_batch* b, const cfd_config* cfg, int recipe, uint64_t seed,
+                         int nbubbles, int max_steps, int* id_out) {
+    if (!b || !cfg || !id_out) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    std::vector<cfdic::Op> ops;
+    cfdic::Eos q;
+    int r = cfdic::recipe_program(cfg, recipe, seed, nbubbles, ops, q);
+    if (r) return cfd_fail(r, "recipe %d does not apply to this configuration", recipe);
+    return add_member(b, cfg, nullptr, &ops, &q, max_steps, id_out);
 }
 
 static Member* find(cfd_batch* b, int id) {

@@ -7,6 +7,12 @@
 // reference's (checked by the tests).  The seeded workload recipes
 // (four-quadrant Riemann problem, shock + bubbles, water shock on an air
 // bubble) are new ICs built from the same helpers.
+//
+// Every recipe and every named case made of the reference's shape helpers is
+// expressed as a shape program (csrc/ic_program.h) that the host evaluates
+// here and the device evaluates in csrc/cfd_ic.cu; the four Allaire cases
+// with their own per-cell formulas (shocked_SF6, TSTM, RMI_SF6,
+// tin_air_implosion) stay host-only.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -16,6 +22,9 @@
 
 #include "../../include/cfdgpu.h"
 #include "../../include/cfdgpu_host.h"
+#include "ic_builders.h"
+
+using cfdic::Op;
 
 namespace {
 
@@ -31,63 +40,102 @@ struct Grid {
     double ccy(int i) const { return y0 + double(i - g) * dy + 0.5 * dy; }
 };
 
-struct Eos1 {
-    double g, p;
-};
-struct Eos2 {
-    double g1, g2, p1, p2;
-};
-
-// E/headers/misc_euler.hpp:83-97
-void euler_p2c(const Eos1& q, const double* W, double* U) {
-    double rho = W[0], u = W[1], v = W[2], p = W[3];
-    double e = (p + q.g * q.p) / ((q.g - 1.0) * rho);
-    U[0] = rho;
-    U[1] = rho * u;
-    U[2] = rho * v;
-    U[3] = rho * e + 0.5 * rho * (u * u + v * v);
-}
-// E/headers/misc_euler.hpp:63-79
-void euler_c2p(const Eos1& q, const double* U, double* W) {
-    double rho = U[0];
-    double u = U[1] / rho;
-    double v = U[2] / rho;
-    double e = U[3] / rho - 0.5 * (u * u + v * v);
-    W[0] = rho;
-    W[1] = u;
-    W[2] = v;
-    W[3] = (q.g - 1.0) * rho * e - q.g * q.p;
-}
-// A/headers/mixturemodel.hpp:26-32 and A/headers/misc.hpp:149-163
-void allaire_p2c(const Eos2& q, const double* W, double* U) {
-    double rho = W[0] + W[1];
-    double z = W[5];
-    double eps = z / (q.g1 - 1.0) + (1.0 - z) / (q.g2 - 1.0);
-    double k = (z * q.g1 * q.p1 / (q.g1 - 1.0) + (1.0 - z) * q.g2 * q.p2 / (q.g2 - 1.0)) / eps;
-    double e = (W[4] + k) * eps / rho;
-    U[0] = W[0];
-    U[1] = W[1];
-    U[2] = rho * W[2];
-    U[3] = rho * W[3];
-    U[4] = rho * e + 0.5 * rho * (W[2] * W[2] + W[3] * W[3]);
-    U[5] = W[5];
-}
-void allaire_p2c6(const Eos2& q, double a, double b, double c, double d, double e, double f,
-                  double* U) {
-    double W[6] = {a, b, c, d, e, f};
-    allaire_p2c(q, W, U);
-}
-// E/headers/stiffened_gas_eos.hpp:73-76
-double sg_specific_ie(double g, double pinf, double p, double rho) {
-    return (p + g * pinf) / ((g - 1.0) * rho);
+Grid make_grid(const cfd_config* cfg, double* grid) {
+    Grid G;
+    G.nx = cfg->nx;
+    G.ny = cfg->ny;
+    G.g = cfg->flux_solver == CFD_FLUX_GODUNOV ? 1 : 2;
+    G.nv = cfd_nvar(cfg->model);
+    G.x0 = cfg->x0;
+    G.y0 = cfg->y0;
+    G.dx = cfg->dx;
+    G.dy = cfg->dy;
+    G.a = grid;
+    return G;
 }
 
-void fill(Grid& G, const double* U) {
+cfdic::Eos make_eos(const cfd_config* cfg) {
+    cfdic::Eos q;
+    q.model = cfg->model == CFD_MODEL_EULER ? 0 : 1;
+    q.g1 = cfg->gamma1;
+    q.p1 = cfg->pinf1;
+    q.g2 = cfg->gamma2;
+    q.p2 = cfg->pinf2;
+    return q;
+}
+
+// Runs a shape program over every cell of the ghosted grid.
+void run_program(Grid& G, const std::vector<Op>& ops, const cfdic::Eos& q) {
+    cfdic::Geom geo{G.x0, G.y0, G.dx, G.dy};
     for (int i = 0; i < G.rows(); ++i)
-        for (int j = 0; j < G.cols(); ++j) memcpy(G.cell(i, j), U, sizeof(double) * G.nv);
+        for (int j = 0; j < G.cols(); ++j)
+            cfdic::eval_cell(ops.data(), (int)ops.size(), q, geo, i - G.g, j - G.g, G.cell(i, j));
 }
 
-// Fraction of N x N sub-cell sample points of cell (i, j) satisfying inside().
+// --------------------------------------------------------- op emitters ---
+struct Prog {
+    const cfdic::Eos& q;
+    std::vector<Op>& ops;
+    int nv() const { return cfdic::nvar(q); }
+    Op& push(int kind, int n = 10) {
+        Op o;
+        memset(&o, 0, sizeof o);
+        o.kind = kind;
+        o.n = n;
+        ops.push_back(o);
+        return ops.back();
+    }
+    void copy(double* dst, const double* src) const { memcpy(dst, src, sizeof(double) * nv()); }
+    void fill(const double* U) { copy(push(cfdic::OP_FILL).v[0], U); }
+    // E/sourcecode/euler_io.cpp:335-389
+    void add_circle(const double* U, double cx, double cy, double R, int N = 10) {
+        Op& o = push(cfdic::OP_ADD_CIRCLE, N);
+        o.a[0] = cx, o.a[1] = cy, o.a[2] = R;
+        copy(o.v[0], U);
+    }
+    // E/sourcecode/euler_io.cpp:282-330
+    void add_rect(const double* U, double blx, double bly, double w, double h, int N = 10) {
+        Op& o = push(cfdic::OP_ADD_RECT, N);
+        o.a[0] = blx, o.a[1] = bly, o.a[2] = w, o.a[3] = h;
+        copy(o.v[0], U);
+    }
+    // E/sourcecode/euler_io.cpp:392-433, A/sourcecode/allaire_diffuse_io.cpp:358-399
+    void set_circular(const double* W_in, const double* W_out, double cx, double cy, double R,
+                      int N) {
+        Op& o = push(cfdic::OP_SET_CIRCULAR, N);
+        o.a[0] = cx, o.a[1] = cy, o.a[2] = R;
+        copy(o.v[0], W_in);
+        copy(o.v[1], W_out);
+    }
+    // A/sourcecode/allaire_diffuse_io.cpp:312-355
+    void set_planar(const double* U_under, const double* U_over, double a, double b, double c) {
+        Op& o = push(cfdic::OP_SET_PLANAR);
+        o.a[0] = a, o.a[1] = b, o.a[2] = c;
+        copy(o.v[0], U_under);
+        copy(o.v[1], U_over);
+    }
+    void set_halfspace(const double* U_under, double a, double b, double c) {
+        Op& o = push(cfdic::OP_SET_HALFSPACE);
+        o.a[0] = a, o.a[1] = b, o.a[2] = c;
+        copy(o.v[0], U_under);
+    }
+    // W = frac W_in + (1 - frac) W(cell), frac from 10 x 10 sub-samples,
+    // cells with frac == 0 untouched.  Unlike add_circle_to_IC this keeps
+    // overlapping bubbles physical.
+    void blend_circle(const double* W_in, double cx, double cy, double R) {
+        Op& o = push(cfdic::OP_BLEND_CIRCLE, 10);
+        o.a[0] = cx, o.a[1] = cy, o.a[2] = R;
+        copy(o.v[0], W_in);
+    }
+    void quadrants(const double U[4][4], double xs, double ys) {
+        Op& o = push(cfdic::OP_QUADRANTS);
+        o.a[0] = xs, o.a[1] = ys;
+        for (int k = 0; k < 4; ++k) copy(o.v[k], U[k]);
+    }
+};
+
+// Fraction of N x N sub-cell sample points of cell (i, j) satisfying inside()
+// (E/sourcecode/euler_io.cpp:300-318), for the per-cell Allaire cases.
 template <class F> double sample_frac(const Grid& G, int i, int j, int N, F inside) {
     int numinside = 0;
     double delx = G.dx / N, dely = G.dy / N;
@@ -101,72 +149,9 @@ template <class F> double sample_frac(const Grid& G, int i, int j, int N, F insi
     return double(numinside) / (N * N);
 }
 
-// E/sourcecode/euler_io.cpp:335-389: adds frac * U_in (cells farther than
-// R + 2 dx from the centre add 0 * U_in).
-void add_circle(Grid& G, const double* U_in, double cx, double cy, double R, int N = 10) {
-    for (int i = 0; i < G.rows(); ++i)
-        for (int j = 0; j < G.cols(); ++j) {
-            double dxc = G.ccx(j) - cx, dyc = G.ccy(i) - cy;
-            double frac;
-            if (std::sqrt(dxc * dxc + dyc * dyc) > R + 2.0 * G.dx) {
-                frac = 0.0;
-            } else {
-                frac = sample_frac(G, i, j, N, [&](double sx, double sy) {
-                    sx -= cx;
-                    sy -= cy;
-                    return std::sqrt(sx * sx + sy * sy) <= R;
-                });
-            }
-            double* c = G.cell(i, j);
-            for (int k = 0; k < G.nv; ++k) c[k] += frac * U_in[k];
-        }
-}
-
-// E/sourcecode/euler_io.cpp:282-330
-void add_rectangle(Grid& G, const double* U_in, double blx, double bly, double w, double h,
-                   int N = 10) {
-    for (int i = 0; i < G.rows(); ++i)
-        for (int j = 0; j < G.cols(); ++j) {
-            double frac = sample_frac(G, i, j, N, [&](double sx, double sy) {
-                sx -= blx;
-                sy -= bly;
-                return (0.0 <= sx) & (sx <= w) & (0.0 <= sy) & (sy <= h);
-            });
-            double* c = G.cell(i, j);
-            for (int k = 0; k < G.nv; ++k) c[k] += frac * U_in[k];
-        }
-}
-
-// E/sourcecode/euler_io.cpp:392-433 and A/sourcecode/allaire_diffuse_io.cpp:358-399:
-// W = frac W_in + (1-frac) W_out, converted per cell.
-template <class P2C>
-void set_circular(Grid& G, const double* W_in, const double* W_out, double cx, double cy, double R,
-                  int N, P2C p2c) {
-    double W[6];
-    for (int i = 0; i < G.rows(); ++i)
-        for (int j = 0; j < G.cols(); ++j) {
-            double frac = sample_frac(G, i, j, N, [&](double sx, double sy) {
-                sx -= cx;
-                sy -= cy;
-                return std::sqrt(sx * sx + sy * sy) <= R;
-            });
-            for (int k = 0; k < G.nv; ++k) W[k] = frac * W_in[k] + (1.0 - frac) * W_out[k];
-            p2c(W, G.cell(i, j));
-        }
-}
-
-// A/sourcecode/allaire_diffuse_io.cpp:312-355
-void set_planar(Grid& G, const double* U_under, const double* U_over, double a, double b,
-                double c) {
-    for (int i = 0; i < G.rows(); ++i)
-        for (int j = 0; j < G.cols(); ++j)
-            memcpy(G.cell(i, j), (G.ccx(j) * a + G.ccy(i) * b <= c) ? U_under : U_over,
-                   sizeof(double) * G.nv);
-}
-void set_halfspace(Grid& G, const double* U_under, double a, double b, double c) {
-    for (int i = 0; i < G.rows(); ++i)
-        for (int j = 0; j < G.cols(); ++j)
-            if (G.ccx(j) * a + G.ccy(i) * b <= c) memcpy(G.cell(i, j), U_under, sizeof(double) * G.nv);
+// E/headers/stiffened_gas_eos.hpp:73-76
+double sg_specific_ie(double g, double pinf, double p, double rho) {
+    return (p + g * pinf) / ((g - 1.0) * rho);
 }
 
 void base_cfg(cfd_config* c, int model, int nx, int ny, int flux_solver) {
@@ -225,28 +210,27 @@ bool euler_params(const std::string& tc, cfd_config* c) {
 }
 
 // E/sourcecode/euler_io.cpp:497-726 (initial states)
-void euler_case_ic(const std::string& tc, const Eos1& q, Grid& G, uint64_t seed) {
+bool euler_case_program(const std::string& tc, Prog& P, uint64_t seed) {
     auto U_of = [&](double r, double u, double v, double p, double* U) {
         double W[4] = {r, u, v, p};
-        euler_p2c(q, W, U);
+        cfdic::euler_p2c(P.q, W, U);
     };
     double Ubg[4], Ui[4];
     U_of(0.125, 0.0, 0.0, 0.1, Ubg);
     auto circ = [&](double r, double p, double cx, double cy, double R) {
         U_of(r, 0.0, 0.0, p, Ui);
-        add_circle(G, Ui, cx, cy, R);
+        P.add_circle(Ui, cx, cy, R);
     };
     auto rect = [&](double r, double p, double bx, double by, double w, double h) {
         U_of(r, 0.0, 0.0, p, Ui);
-        add_rectangle(G, Ui, bx, by, w, h);
+        P.add_rect(Ui, bx, by, w, h);
     };
     if (tc == "circular_explosion") {
         double Win[4] = {1.0, 0.0, 0.0, 1.0}, Wout[4] = {0.125, 0.0, 0.0, 0.1};
-        set_circular(G, Win, Wout, 1.0, 1.0, 0.4, 10,
-                     [&](const double* W, double* U) { euler_p2c(q, W, U); });
-        return;
+        P.set_circular(Win, Wout, 1.0, 1.0, 0.4, 10);
+        return true;
     }
-    fill(G, Ubg);
+    P.fill(Ubg);
     if (tc == "multiple_circles_1") {
         const double c[9][2] = {{0.5, 0.4}, {0.3, 0.7}, {0.2, 0.7}, {0.6, 0.5}, {0.1, 0.3},
                                 {0.3, 0.5}, {0.4, 0.6}, {0.5, 0.4}, {0.5, 0.3}};
@@ -317,7 +301,10 @@ void euler_case_ic(const std::string& tc, const Eos1& q, Grid& G, uint64_t seed)
                 double density = 5.0 * dis(gen);
                 circ(density, density, cx, cy, 0.02);
             }
+    } else {
+        return false;
     }
+    return true;
 }
 
 // -------------------------------------------------------------- Allaire ---
@@ -374,76 +361,91 @@ void mixed_cell(double z, double rho1, double rho2, double u, double v, double e
     U[5] = z;
 }
 
-bool allaire_case_ic(const std::string& tc, const Eos2& q, Grid& G) {
-    auto P = [&](double a, double b, double c, double d, double e, double f, double* U) {
-        allaire_p2c6(q, a, b, c, d, e, f, U);
+bool allaire_per_cell_case(const std::string& tc) {
+    return tc == "shocked_SF6" || tc == "TSTM" || tc == "RMI_SF6" || tc == "tin_air_implosion";
+}
+
+// A/sourcecode/allaire_diffuse_io.cpp:401-640 (initial states built from
+// the shape helpers)
+bool allaire_case_program(const std::string& tc, Prog& P) {
+    auto Pc = [&](double a, double b, double c, double d, double e, double f, double* U) {
+        double W[6] = {a, b, c, d, e, f};
+        cfdic::allaire_p2c(P.q, W, U);
     };
-    auto p2c = [&](const double* W, double* U) { allaire_p2c(q, W, U); };
+    auto p2c = [&](const double* W, double* U) { cfdic::allaire_p2c(P.q, W, U); };
     double Ul[6], Ur[6];
     bool xdir = tc.find("_x") != std::string::npos;
     auto planar = [&]() {
-        if (xdir) set_planar(G, Ul, Ur, 1.0, 0.0, 0.5);
-        else set_planar(G, Ul, Ur, 0.0, 1.0, 0.5);
+        if (xdir) P.set_planar(Ul, Ur, 1.0, 0.0, 0.5);
+        else P.set_planar(Ul, Ur, 0.0, 1.0, 0.5);
     };
     if (tc == "ST1_x" || tc == "ST1_y") {
-        P(1.0, 0.0, 0.0, 0.0, 1.0, 1.0, Ul);
-        P(0.0, 0.125, 0.0, 0.0, 0.1, 0.0, Ur);
+        Pc(1.0, 0.0, 0.0, 0.0, 1.0, 1.0, Ul);
+        Pc(0.0, 0.125, 0.0, 0.0, 0.1, 0.0, Ur);
         planar();
     } else if (tc == "ST2_x" || tc == "ST2_y") {
-        P(1000.0, 0.0, 0.0, 0.0, 1000000000.0, 1.0, Ul);
-        P(0.0, 50.0, 0.0, 0.0, 100000.0, 0.0, Ur);
-        if (xdir) set_planar(G, Ul, Ur, 1.0, 0.0, 0.7);
-        else set_planar(G, Ul, Ur, 0.0, 1.0, 0.7);
+        Pc(1000.0, 0.0, 0.0, 0.0, 1000000000.0, 1.0, Ul);
+        Pc(0.0, 50.0, 0.0, 0.0, 100000.0, 0.0, Ur);
+        if (xdir) P.set_planar(Ul, Ur, 1.0, 0.0, 0.7);
+        else P.set_planar(Ul, Ur, 0.0, 1.0, 0.7);
     } else if (tc == "TTC5_x_pure" || tc == "TTC5_y_pure") {
-        P(5.99924, 0.0, 19.5975, 0.0, 460.894, 1.0, Ul);
-        P(5.99242, 0.0, -6.19633, 0.0, 46.0950, 1.0, Ur);
+        Pc(5.99924, 0.0, 19.5975, 0.0, 460.894, 1.0, Ul);
+        Pc(5.99242, 0.0, -6.19633, 0.0, 46.0950, 1.0, Ur);
         planar();
     } else if (tc == "TTC1_x_pure" || tc == "TTC1_y_pure") {
-        P(1.0, 0.0, 0.0, 0.0, 1.0, 1.0, Ul);
-        P(0.125, 0.0, 0.0, 0.0, 0.1, 1.0, Ur);
+        Pc(1.0, 0.0, 0.0, 0.0, 1.0, 1.0, Ul);
+        Pc(0.125, 0.0, 0.0, 0.0, 0.1, 1.0, Ur);
         planar();
     } else if (tc == "TTC2_x_pure" || tc == "TTC2_y_pure") {
-        P(1.0, 0.0, -2.0, 0.0, 0.4, 1.0, Ul);
-        P(1.0, 0.0, 2.0, 0.0, 0.4, 1.0, Ur);
+        Pc(1.0, 0.0, -2.0, 0.0, 0.4, 1.0, Ul);
+        Pc(1.0, 0.0, 2.0, 0.0, 0.4, 1.0, Ur);
         planar();
     } else if (tc == "TTC3_x_pure" || tc == "TTC3_y_pure") {
-        P(1.0, 0.0, 0.0, 0.0, 1000.0, 1.0, Ul);
-        P(1.0, 0.0, 0.0, 0.0, 0.01, 1.0, Ur);
+        Pc(1.0, 0.0, 0.0, 0.0, 1000.0, 1.0, Ul);
+        Pc(1.0, 0.0, 0.0, 0.0, 0.01, 1.0, Ur);
         planar();
     } else if (tc == "TTC4_x_pure" || tc == "TTC4_y_pure") {
-        P(1.0, 0.0, 0.0, 0.0, 0.1, 1.0, Ul);
-        P(1.0, 0.0, 0.0, 0.0, 100.0, 1.0, Ur);
+        Pc(1.0, 0.0, 0.0, 0.0, 0.1, 1.0, Ul);
+        Pc(1.0, 0.0, 0.0, 0.0, 100.0, 1.0, Ur);
         planar();
     } else if (tc == "circular_explosion") {
         double Win[6] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0}, Wout[6] = {0.0, 0.125, 0.0, 0.0, 0.1, 0.0};
-        set_circular(G, Win, Wout, 1.0, 1.0, 0.4, 10, p2c);
+        P.set_circular(Win, Wout, 1.0, 1.0, 0.4, 10);
     } else if (tc == "shocked_helium_bubble") {
         double Wh[6] = {0.0, 0.138, 0.0, 0.0, 1.0, 0.0}, Wpre[6] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0};
         double Wpost[6] = {1.3764, 0.0, -0.394, 0.0, 1.5698, 1.0};
-        set_circular(G, Wh, Wpre, 175.0, 44.5, 25.0, 10, p2c);
+        P.set_circular(Wh, Wpre, 175.0, 44.5, 25.0, 10);
         p2c(Wpost, Ul);
-        set_halfspace(G, Ul, -1.0, 0.0, -225.0);
+        P.set_halfspace(Ul, -1.0, 0.0, -225.0);
     } else if (tc == "shocked_R22_bubble") {
         double Wr[6] = {0.0, 3.863, 0.0, 0.0, 1.01325e5, 0.0};
         double Wpre[6] = {1.225, 0.0, 0.0, 0.0, 1.01325e5, 1.0};
         double Wpost[6] = {1.686, 0.0, -113.5, 0.0, 1.59e5, 1.0};
-        set_circular(G, Wr, Wpre, 0.225, 0.0445, 0.025, 25, p2c);
+        P.set_circular(Wr, Wpre, 0.225, 0.0445, 0.025, 25);
         p2c(Wpost, Ul);
-        set_halfspace(G, Ul, -1.0, 0.0, -0.275);
+        P.set_halfspace(Ul, -1.0, 0.0, -0.275);
     } else if (tc == "underwater_shocked_bubble") {
         double Wa[6] = {0.0, 0.0012, 0.0, 0.0, 1.0, 0.0}, Wpre[6] = {1.0, 0.0, 0.0, 0.0, 1.0, 1.0};
         double Wpost[6] = {1.31, 0.0, 67.32, 0.0, 19000.0, 1.0};
-        set_circular(G, Wa, Wpre, 6.0, 6.0, 3.0, 10, p2c);
+        P.set_circular(Wa, Wpre, 6.0, 6.0, 3.0, 10);
         p2c(Wpost, Ul);
-        set_halfspace(G, Ul, 1.0, 0.0, 2.4);
+        P.set_halfspace(Ul, 1.0, 0.0, 2.4);
     } else if (tc == "underwater_explosion" || tc == "underwater_explosion_modified") {
         double Ww[6] = {0.0, 1000.0, 0.0, 0.0, 1.0e5, 0.0}, Wa[6] = {1.0, 0.0, 0.0, 0.0, 1.0e5, 1.0};
         double Wb[6] = {1270.0, 0.0, 0.0, 0.0, 8.29e8, 1.0};
-        set_circular(G, Wb, Ww, 0.0, 0.0, 1.0, 10, p2c);
+        P.set_circular(Wb, Ww, 0.0, 0.0, 1.0, 10);
         p2c(Wa, Ul);
-        set_halfspace(G, Ul, 0.0, -1.0, -2.5);
-    } else if (tc == "shocked_SF6" || tc == "TSTM" || tc == "RMI_SF6") {
-        // A/sourcecode/allaire_diffuse_io.cpp:640-900: z from sub-sampled shapes
+        P.set_halfspace(Ul, 0.0, -1.0, -2.5);
+    } else {
+        return false;
+    }
+    return true;
+}
+
+// A/sourcecode/allaire_diffuse_io.cpp:640-983: the cases whose volume
+// fraction comes from a per-cell formula (host only).
+void allaire_per_cell_ic(const std::string& tc, const cfdic::Eos& q, Grid& G) {
+    if (tc == "shocked_SF6" || tc == "TSTM" || tc == "RMI_SF6") {
         double rpre, ppre, upre, rpost, ppost, upost, rho2, p2;
         if (tc == "shocked_SF6") {
             rpre = 1.153; ppre = 9.6856; upre = 0.0;
@@ -492,7 +494,6 @@ bool allaire_case_ic(const std::string& tc, const Eos2& q, Grid& G) {
                 mixed_cell(z, rho1, rho2, u, v, e1, e2, G.cell(i, j));
             }
     } else if (tc == "tin_air_implosion") {
-        // A/sourcecode/allaire_diffuse_io.cpp:900-983
         double rpre = 7.28, ppre = 1.0, rpost = 11.84, ppost = 1000000.0;
         double epre = sg_specific_ie(q.g1, q.p1, ppre, rpre);
         double epost = sg_specific_ie(q.g1, q.p1, ppost, rpost);
@@ -514,10 +515,7 @@ bool allaire_case_ic(const std::string& tc, const Eos2& q, Grid& G) {
                 });
                 mixed_cell(1.0 - frac, rho1, rho2, 0.0, 0.0, e1, e2, G.cell(i, j));
             }
-    } else {
-        return false;
     }
-    return true;
 }
 
 // ------------------------------------------------------------- recipes ---
@@ -529,34 +527,102 @@ struct Rng {
     double range(double a, double b) { return a + (b - a) * u(); }
 };
 
-// Blends a circular region into the current state:
-// W = frac * W_in + (1 - frac) * W(cell), frac from 10 x 10 sub-samples,
-// cells with frac == 0 untouched.  Unlike add_circle_to_IC this keeps
-// overlapping bubbles physical.
-template <class P2C, class C2P>
-void blend_circle(Grid& G, const double* W_in, double cx, double cy, double R, P2C p2c, C2P c2p) {
-    double reach = R + 2.0 * std::fmax(G.dx, G.dy);
-    int j0 = std::max(0, (int)std::floor((cx - reach - G.x0) / G.dx) + G.g - 1);
-    int j1 = std::min(G.cols() - 1, (int)std::ceil((cx + reach - G.x0) / G.dx) + G.g + 1);
-    int i0 = std::max(0, (int)std::floor((cy - reach - G.y0) / G.dy) + G.g - 1);
-    int i1 = std::min(G.rows() - 1, (int)std::ceil((cy + reach - G.y0) / G.dy) + G.g + 1);
-    double W[6];
-    for (int i = i0; i <= i1; ++i)
-        for (int j = j0; j <= j1; ++j) {
-            double frac = sample_frac(G, i, j, 10, [&](double sx, double sy) {
-                sx -= cx;
-                sy -= cy;
-                return std::sqrt(sx * sx + sy * sy) <= R;
-            });
-            if (frac == 0.0) continue;
-            double* c = G.cell(i, j);
-            c2p(c, W);
-            for (int k = 0; k < G.nv; ++k) W[k] = frac * W_in[k] + (1.0 - frac) * W[k];
-            p2c(W, c);
+bool recipe_program(const cfd_config* cfg, int recipe, uint64_t seed, int nbubbles, Prog& P) {
+    if (recipe == CFD_RECIPE_FOUR_QUADRANT) {
+        // 2D Riemann problem split at (0.5, 0.5): quadrants (x>1/2,y>1/2),
+        // (x<1/2,y>1/2), (x<1/2,y<1/2), (x>1/2,y<1/2), by cell centre.
+        const double Wq[4][4] = {{1.5, 0.0, 0.0, 1.5},
+                                 {0.5323, 1.206, 0.0, 0.3},
+                                 {0.138, 1.206, 1.206, 0.029},
+                                 {0.5323, 0.0, 1.206, 0.3}};
+        double Uq[4][4];
+        for (int k = 0; k < 4; ++k) cfdic::euler_p2c(P.q, Wq[k], Uq[k]);
+        P.quadrants(Uq, 0.5, 0.5);
+        return true;
+    }
+    if (recipe == CFD_RECIPE_SHOCK_BUBBLES) {
+        // Background rho = 1, p = 1 at rest; bubbles of log-uniform density
+        // at p = 1 blended in; a Mach-2 shock at x = 0.1 moving +x with the
+        // Rankine-Hugoniot post-shock state of gamma = 1.4.
+        double Wbg[4] = {1.0, 0.0, 0.0, 1.0}, Ubg[4];
+        cfdic::euler_p2c(P.q, Wbg, Ubg);
+        P.fill(Ubg);
+        Rng r(seed);
+        for (int b = 0; b < nbubbles; ++b) {
+            double cx = r.range(0.2, 1.0), cy = r.u();
+            double R = r.range(0.02, 0.08);
+            double rho = std::exp(r.range(std::log(0.1), std::log(10.0)));
+            double Wb[4] = {rho, 0.0, 0.0, 1.0};
+            P.blend_circle(Wb, cx, cy, R);
         }
+        double g = cfg->gamma1, M = 2.0;
+        double rho2 = (g + 1.0) * M * M / ((g - 1.0) * M * M + 2.0);
+        double p2 = 1.0 + 2.0 * g / (g + 1.0) * (M * M - 1.0);
+        double u2 = M * std::sqrt(g) * (1.0 - 1.0 / rho2);
+        double Wp[4] = {rho2, u2, 0.0, p2}, Up[4];
+        cfdic::euler_p2c(P.q, Wp, Up);
+        P.set_halfspace(Up, 1.0, 0.0, 0.1);
+        return true;
+    }
+    if (recipe == CFD_RECIPE_WATER_SHOCK_AIR_BUBBLE) {
+        // Water (material 1, z = 1 - z_min) at 1e5 Pa with an air bubble
+        // (z = z_min) of radius U[0.1, 0.2] centred in [0.6,1.4]x[0.3,0.7];
+        // a planar water shock at x = 0.2 with 1e9 Pa behind it and the
+        // stiffened-gas Rankine-Hugoniot post-shock state.
+        double zm = cfg->z_min > 0.0 ? cfg->z_min : 1e-6;
+        double rho_w = 1000.0, rho_a = 1.0, p0 = 1e5, p1 = 1e9;
+        Rng r(seed);
+        double cx = r.range(0.6, 1.4), cy = r.range(0.3, 0.7), R = r.range(0.1, 0.2);
+        double zw = 1.0 - zm, za = zm;
+        double Ww[6] = {zw * rho_w, (1.0 - zw) * rho_a, 0.0, 0.0, p0, zw};
+        double Wa[6] = {za * rho_w, (1.0 - za) * rho_a, 0.0, 0.0, p0, za};
+        P.set_circular(Wa, Ww, cx, cy, R, 10);
+        double gw = cfg->gamma1, pi = cfg->pinf1;
+        double a1 = p0 + pi, a2 = p1 + pi;
+        double ratio = ((gw + 1.0) * a2 + (gw - 1.0) * a1) / ((gw - 1.0) * a2 + (gw + 1.0) * a1);
+        double rho_s = rho_w * ratio;
+        double u_s = std::sqrt((p1 - p0) * (1.0 / rho_w - 1.0 / rho_s));
+        double Ws[6] = {zw * rho_s, (1.0 - zw) * rho_a, u_s, 0.0, p1, zw}, Us[6];
+        cfdic::allaire_p2c(P.q, Ws, Us);
+        P.set_halfspace(Us, 1.0, 0.0, 0.2);
+        return true;
+    }
+    return false;
+}
+
+bool recipe_model_ok(const cfd_config* cfg, int recipe) {
+    int want = recipe == CFD_RECIPE_WATER_SHOCK_AIR_BUBBLE ? CFD_MODEL_ALLAIRE : CFD_MODEL_EULER;
+    return cfg->model == want;
 }
 
 }  // namespace
+
+namespace cfdic {
+
+int case_program(const cfd_config* cfg, const char* test_case, uint64_t seed,
+                 std::vector<Op>& ops, Eos& q) {
+    if (!cfg || !test_case) return CFD_ERR_INVALID;
+    ops.clear();
+    q = make_eos(cfg);
+    std::string tc = test_case;
+    Prog P{q, ops};
+    if (cfg->model == CFD_MODEL_EULER) return euler_case_program(tc, P, seed) ? CFD_OK : CFD_ERR_INVALID;
+    if (!allaire_lookup(tc)) return CFD_ERR_INVALID;
+    if (allaire_per_cell_case(tc)) return CFD_ERR_UNSUPPORTED;
+    return allaire_case_program(tc, P) ? CFD_OK : CFD_ERR_INVALID;
+}
+
+int recipe_program(const cfd_config* cfg, int recipe, uint64_t seed, int nbubbles,
+                   std::vector<Op>& ops, Eos& q) {
+    if (!cfg) return CFD_ERR_INVALID;
+    ops.clear();
+    q = make_eos(cfg);
+    if (!recipe_model_ok(cfg, recipe)) return CFD_ERR_INVALID;
+    Prog P{q, ops};
+    return ::recipe_program(cfg, recipe, seed, nbubbles, P) ? CFD_OK : CFD_ERR_INVALID;
+}
+
+}  // namespace cfdic
 
 extern "C" {
 
@@ -590,25 +656,18 @@ int cfd_case_config(int model, const char* test_case, int nx, int ny, int flux_s
 
 int cfd_case_ic(const cfd_config* cfg, const char* test_case, uint64_t seed, double* grid) {
     if (!cfg || !test_case || !grid) return CFD_ERR_INVALID;
-    Grid G;
-    G.nx = cfg->nx;
-    G.ny = cfg->ny;
-    G.g = cfg->flux_solver == CFD_FLUX_GODUNOV ? 1 : 2;
-    G.nv = cfd_nvar(cfg->model);
-    G.x0 = cfg->x0;
-    G.y0 = cfg->y0;
-    G.dx = cfg->dx;
-    G.dy = cfg->dy;
-    G.a = grid;
+    Grid G = make_grid(cfg, grid);
     memset(grid, 0, sizeof(double) * G.nv * G.rows() * G.cols());
-    std::string tc = test_case;
-    if (cfg->model == CFD_MODEL_EULER) {
-        Eos1 q{cfg->gamma1, cfg->pinf1};
-        euler_case_ic(tc, q, G, seed);
+    std::vector<Op> ops;
+    cfdic::Eos q;
+    int r = cfdic::case_program(cfg, test_case, seed, ops, q);
+    if (r == CFD_ERR_UNSUPPORTED) {
+        allaire_per_cell_ic(test_case, q, G);
         return CFD_OK;
     }
-    Eos2 q{cfg->gamma1, cfg->gamma2, cfg->pinf1, cfg->pinf2};
-    return allaire_case_ic(tc, q, G) ? CFD_OK : CFD_ERR_INVALID;
+    if (r) return r;
+    run_program(G, ops, q);
+    return CFD_OK;
 }
 
 int cfd_recipe_config(int recipe, int nx, int ny, cfd_config* cfg) {
@@ -653,85 +712,13 @@ int cfd_recipe_config(int recipe, int nx, int ny, cfd_config* cfg) {
 
 int cfd_recipe_ic(const cfd_config* cfg, int recipe, uint64_t seed, int nbubbles, double* grid) {
     if (!cfg || !grid) return CFD_ERR_INVALID;
-    Grid G;
-    G.nx = cfg->nx;
-    G.ny = cfg->ny;
-    G.g = cfg->flux_solver == CFD_FLUX_GODUNOV ? 1 : 2;
-    G.nv = cfd_nvar(cfg->model);
-    G.x0 = cfg->x0;
-    G.y0 = cfg->y0;
-    G.dx = cfg->dx;
-    G.dy = cfg->dy;
-    G.a = grid;
-    if (recipe == CFD_RECIPE_FOUR_QUADRANT) {
-        // 2D Riemann problem split at (0.5, 0.5): quadrants (x>1/2,y>1/2),
-        // (x<1/2,y>1/2), (x<1/2,y<1/2), (x>1/2,y<1/2), by cell centre.
-        Eos1 q{cfg->gamma1, cfg->pinf1};
-        const double Wq[4][4] = {{1.5, 0.0, 0.0, 1.5},
-                                 {0.5323, 1.206, 0.0, 0.3},
-                                 {0.138, 1.206, 1.206, 0.029},
-                                 {0.5323, 0.0, 1.206, 0.3}};
-        double Uq[4][4];
-        for (int k = 0; k < 4; ++k) euler_p2c(q, Wq[k], Uq[k]);
-        for (int i = 0; i < G.rows(); ++i)
-            for (int j = 0; j < G.cols(); ++j) {
-                bool right = G.ccx(j) > 0.5, top = G.ccy(i) > 0.5;
-                int k = top ? (right ? 0 : 1) : (right ? 3 : 2);
-                memcpy(G.cell(i, j), Uq[k], sizeof(double) * 4);
-            }
-        return CFD_OK;
-    }
-    if (recipe == CFD_RECIPE_SHOCK_BUBBLES) {
-        // Background rho = 1, p = 1 at rest; bubbles of log-uniform density
-        // at p = 1 blended in; a Mach-2 shock at x = 0.1 moving +x with the
-        // Rankine-Hugoniot post-shock state of gamma = 1.4.
-        Eos1 q{cfg->gamma1, cfg->pinf1};
-        double Wbg[4] = {1.0, 0.0, 0.0, 1.0}, Ubg[4];
-        euler_p2c(q, Wbg, Ubg);
-        fill(G, Ubg);
-        Rng r(seed);
-        for (int b = 0; b < nbubbles; ++b) {
-            double cx = r.range(0.2, 1.0), cy = r.u();
-            double R = r.range(0.02, 0.08);
-            double rho = std::exp(r.range(std::log(0.1), std::log(10.0)));
-            double Wb[4] = {rho, 0.0, 0.0, 1.0};
-            blend_circle(G, Wb, cx, cy, R, [&](const double* W, double* U) { euler_p2c(q, W, U); },
-                         [&](const double* U, double* W) { euler_c2p(q, U, W); });
-        }
-        double g = cfg->gamma1, M = 2.0;
-        double rho2 = (g + 1.0) * M * M / ((g - 1.0) * M * M + 2.0);
-        double p2 = 1.0 + 2.0 * g / (g + 1.0) * (M * M - 1.0);
-        double u2 = M * std::sqrt(g) * (1.0 - 1.0 / rho2);
-        double Wp[4] = {rho2, u2, 0.0, p2}, Up[4];
-        euler_p2c(q, Wp, Up);
-        set_halfspace(G, Up, 1.0, 0.0, 0.1);
-        return CFD_OK;
-    }
-    if (recipe == CFD_RECIPE_WATER_SHOCK_AIR_BUBBLE) {
-        // Water (material 1, z = 1 - z_min) at 1e5 Pa with an air bubble
-        // (z = z_min) of radius U[0.1, 0.2] centred in [0.6,1.4]x[0.3,0.7];
-        // a planar water shock at x = 0.2 with 1e9 Pa behind it and the
-        // stiffened-gas Rankine-Hugoniot post-shock state.
-        Eos2 q{cfg->gamma1, cfg->gamma2, cfg->pinf1, cfg->pinf2};
-        double zm = cfg->z_min > 0.0 ? cfg->z_min : 1e-6;
-        double rho_w = 1000.0, rho_a = 1.0, p0 = 1e5, p1 = 1e9;
-        Rng r(seed);
-        double cx = r.range(0.6, 1.4), cy = r.range(0.3, 0.7), R = r.range(0.1, 0.2);
-        double zw = 1.0 - zm, za = zm;
-        double Ww[6] = {zw * rho_w, (1.0 - zw) * rho_a, 0.0, 0.0, p0, zw};
-        double Wa[6] = {za * rho_w, (1.0 - za) * rho_a, 0.0, 0.0, p0, za};
-        set_circular(G, Wa, Ww, cx, cy, R, 10, [&](const double* W, double* U) { allaire_p2c(q, W, U); });
-        double gw = cfg->gamma1, pi = cfg->pinf1;
-        double a1 = p0 + pi, a2 = p1 + pi;
-        double ratio = ((gw + 1.0) * a2 + (gw - 1.0) * a1) / ((gw - 1.0) * a2 + (gw + 1.0) * a1);
-        double rho_s = rho_w * ratio;
-        double u_s = std::sqrt((p1 - p0) * (1.0 / rho_w - 1.0 / rho_s));
-        double Ws[6] = {zw * rho_s, (1.0 - zw) * rho_a, u_s, 0.0, p1, zw}, Us[6];
-        allaire_p2c(q, Ws, Us);
-        set_halfspace(G, Us, 1.0, 0.0, 0.2);
-        return CFD_OK;
-    }
-    return CFD_ERR_INVALID;
+    Grid G = make_grid(cfg, grid);
+    std::vector<Op> ops;
+    cfdic::Eos q;
+    int r = cfdic::recipe_program(cfg, recipe, seed, nbubbles, ops, q);
+    if (r) return r;
+    run_program(G, ops, q);
+    return CFD_OK;
 }
 
 }  // extern "C"

@@ -42,6 +42,9 @@ struct Request {
     int64_t id;
     cfd_config cfg;
     std::vector<double> ic;   // ghosted AoS initial grid; reused for the result
+    int recipe = 0;           // > 0: initial condition built on the device at admission
+    uint64_t seed = 0;
+    int nbubbles = 0;
     int steps;
     int state = CFD_REQ_QUEUED;
     int error = 0;
@@ -137,13 +140,19 @@ void worker_main(cfd_server* s) {
         for (Request* r : start) {
             int rc;
             if (s->opt.precision == CFD_PREC_MIXED) {
-                rc = cfd_batch_add(s->batch, &r->cfg, r->ic.data(), r->steps, &r->member);
+                rc = r->recipe ? cfd_batch_add_recipe(s->batch, &r->cfg, r->recipe, r->seed,
+                                                      r->nbubbles, r->steps, &r->member)
+                               : cfd_batch_add(s->batch, &r->cfg, r->ic.data(), r->steps,
+                                               &r->member);
             } else {
                 cfd_config c = r->cfg;
                 c.stream = s->stream;
-                c.T = r->cfg.T;
                 rc = cfd_create(&c, &r->solver);
-                if (!rc) rc = cfd_upload(r->solver, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS, 0, 0.0);
+                if (!rc)
+                    rc = r->recipe ? cfd_upload_recipe(r->solver, r->recipe, r->seed, r->nbubbles,
+                                                       0, 0.0)
+                                   : cfd_upload(r->solver, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS,
+                                                0, 0.0);
             }
             std::lock_guard<std::mutex> lk(s->mu);
             if (rc) {
@@ -186,6 +195,11 @@ void worker_main(cfd_server* s) {
         }
         for (Request* r : done) {
             int rc;
+            if (r->ic.empty()) {  // device-built initial condition: room for the result
+                size_t elems = 0;
+                cfd_ic_grid_elems(&r->cfg, &elems);
+                r->ic.resize(elems);
+            }
             if (s->opt.precision == CFD_PREC_MIXED) {
                 rc = cfd_batch_download(s->batch, r->member, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS);
                 cfd_batch_remove(s->batch, r->member);
@@ -209,6 +223,27 @@ void worker_main(cfd_server* s) {
         }
         if (!done.empty()) s->cv_done.notify_all();
     }
+}
+
+}  // namespace
+
+namespace {
+
+int enqueue(cfd_server* s, std::unique_ptr<Request> r, int64_t* id_out) {
+    r->t_submit = Clock::now();
+    const cfd_config* cfg = &r->cfg;
+    size_t need = 0;
+    if (s->opt.precision == CFD_PREC_MIXED) cfd_batch_member_bytes(cfg, &need);
+    else need = fp64_bytes(*cfg);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (need > s->budget)
+        return cfd_fail(CFD_ERR_BUDGET, "request needs %zu bytes, the budget is %zu", need, s->budget);
+    r->id = s->next_id++;
+    *id_out = r->id;
+    s->queue.push_back(r->id);
+    s->reqs[r->id] = std::move(r);
+    s->cv_work.notify_one();
+    return CFD_OK;
 }
 
 }  // namespace
@@ -258,19 +293,21 @@ int cfd_server_submit(cfd_server* s, const cfd_config* cfg, const double* ic, in
     r->cfg.stream = nullptr;
     r->ic.assign(ic, ic + elems);
     r->steps = steps;
-    r->t_submit = Clock::now();
-    size_t need = 0;
-    if (s->opt.precision == CFD_PREC_MIXED) cfd_batch_member_bytes(cfg, &need);
-    else need = fp64_bytes(*cfg);
-    std::lock_guard<std::mutex> lk(s->mu);
-    if (need > s->budget)
-        return cfd_fail(CFD_ERR_BUDGET, "request needs %zu bytes, the budget is %zu", need, s->budget);
-    r->id = s->next_id++;
-    *id_out = r->id;
-    s->queue.push_back(r->id);
-    s->reqs[r->id] = std::move(r);
-    s->cv_work.notify_one();
-    return CFD_OK;
+    return enqueue(s, std::move(r), id_out);
+}
+
+int cfd_server_submit_recipe(cfd_server* s, const cfd_config* cfg, int recipe, uint64_t seed,
+                             int nbubbles, int steps, int64_t* id_out) {
+    if (!s || !cfg || !id_out || steps <= 0 || recipe <= 0)
+        return cfd_fail(CFD_ERR_INVALID, "bad argument");
+    auto r = std::make_unique<Request>();
+    r->cfg = *cfg;
+    r->cfg.stream = nullptr;
+    r->recipe = recipe;
+    r->seed = seed;
+    r->nbubbles = nbubbles;
+    r->steps = steps;
+    return enqueue(s, std::move(r), id_out);
 }
 
 int cfd_server_wait(cfd_server* s, int64_t id, double timeout_s, cfd_request_info* info,

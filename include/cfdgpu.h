@@ -116,6 +116,18 @@ int cfd_upload(cfd_solver* s, const double* host, int layout, int n, double t);
 /* Same from device memory (SoA planes of nx*ny doubles each, nvar planes). */
 int cfd_upload_device(cfd_solver* s, const double* dev_soa, int n, double t);
 
+/* Builds the initial condition on the device, straight into the solver's
+ * state: a seeded recipe (CFD_RECIPE_*, declared in cfdgpu_host.h) or a named
+ * reference test case (set_ICs, sourcecode/euler_io.cpp:436-731 and
+ * A/sourcecode/allaire_diffuse_io.cpp:401-640).  The result is bit-identical
+ * to cfd_recipe_ic / cfd_case_ic followed by cfd_upload, without a host grid
+ * or a host-to-device copy of the state.  The four Allaire cases with
+ * per-cell formulas (shocked_SF6, TSTM, RMI_SF6, tin_air_implosion) return
+ * CFD_ERR_UNSUPPORTED: build them with cfd_case_ic.  No counterpart in the
+ * reference, which builds every grid on the host. */
+int cfd_upload_recipe(cfd_solver* s, int recipe, uint64_t seed, int nbubbles, int n, double t);
+int cfd_upload_case(cfd_solver* s, const char* test_case, uint64_t seed, int n, double t);
+
 /* Copies the current state to the host in `layout`.  In the ghosted layout
  * the ghost strips hold the boundary fill of the current state. */
 int cfd_download(cfd_solver* s, double* host, int layout);
@@ -200,6 +212,10 @@ int cfd_batch_member_bytes(const cfd_config* cfg, size_t* bytes);
  * naive); max_steps <= 0 runs to T.  Synchronous; returns the member id. */
 int cfd_batch_add(cfd_batch* b, const cfd_config* cfg, const double* host_ic, int max_steps,
                   int* id_out);
+/* Same with the initial condition built on the device from a seeded recipe
+ * (see cfd_upload_recipe). */
+int cfd_batch_add_recipe(cfd_batch* b, const cfd_config* cfg, int recipe, uint64_t seed,
+                         int nbubbles, int max_steps, int* id_out);
 int cfd_batch_remove(cfd_batch* b, int id);
 int cfd_batch_size(cfd_batch* b, int* count, size_t* used_bytes, size_t* budget_bytes);
 /* Advances every member by `ticks` steps (members that are done idle). */
@@ -258,6 +274,10 @@ int cfd_server_create(const cfd_server_options* opt, cfd_server** out);
  * grid, which is copied; CFD_ERR_BUDGET if it can never fit. */
 int cfd_server_submit(cfd_server* s, const cfd_config* cfg, const double* ic, int steps,
                       int64_t* id);
+/* Queues a solve whose initial condition is a seeded recipe, built on the
+ * device at admission (no host grid is held while it waits). */
+int cfd_server_submit_recipe(cfd_server* s, const cfd_config* cfg, int recipe, uint64_t seed,
+                             int nbubbles, int steps, int64_t* id);
 /* Waits up to timeout_s (< 0: forever) for a request; on completion fills
  * info and copies the final ghosted grid to `result` (may be NULL). */
 int cfd_server_wait(cfd_server* s, int64_t id, double timeout_s, cfd_request_info* info,
