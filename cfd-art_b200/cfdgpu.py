@@ -26,7 +26,7 @@ LIMITERS = {"minmod": 0, "vanleer": 1, "mc": 2, "unlimited": 3}
 FLUX = {"MUSCL": 0, "Godunov": 1}
 SPLIT = {"naive": 0, "strang": 1}
 WAVESPEED = {"davis": 0, "pvrs": 1}
-GHOSTED_AOS, SOA = 0, 1
+GHOSTED_AOS, SOA, GHOSTED_AOS_AS_REFERENCE = 0, 1, 2
 RECIPE = {"four_quadrant": 1, "shock_bubbles": 2, "water_shock_air_bubble": 3}
 COUNTERS = ["unphysical_input", "slope_zeroed", "first_order", "fixup", "unphysical_output"]
 
@@ -75,6 +75,18 @@ class Status(C.Structure):
 
     def counter_dict(self) -> dict[str, int]:
         return {k: int(self.counters[i]) for i, k in enumerate(COUNTERS)}
+
+
+class Settings(C.Structure):
+    """cfd_settings (include/cfdgpu_host.h)."""
+    _fields_ = [("Nx", C.c_int), ("Ny", C.c_int), ("CFL", C.c_double),
+                ("splitting_scheme", C.c_char * 64), ("test_case", C.c_char * 128),
+                ("output_freq", C.c_int), ("outputpath", C.c_char * 512),
+                ("basename", C.c_char * 768), ("flux_solver", C.c_char * 32),
+                ("riemann_solver", C.c_char * 32), ("problem", C.c_char * 32),
+                ("precision", C.c_char * 16), ("limiter", C.c_char * 16),
+                ("wavespeed", C.c_char * 16), ("steps", C.c_int), ("alpha_clip", C.c_double),
+                ("fix_dy_halfstep", C.c_int), ("seed", C.c_uint64), ("nbubbles", C.c_int)]
 
 
 class ServerOptions(C.Structure):
@@ -127,6 +139,7 @@ def lib() -> C.CDLL:
             "cfd_advance": (ip, [vp, ip]),
             "cfd_get_status": (ip, [vp, C.POINTER(Status)]),
             "cfd_reset_counters": (ip, [vp]),
+            "cfd_set_reference_ghosts": (ip, [vp, ip]),
             "cfd_set_kernel_timing": (ip, [vp, ip]),
             "cfd_kernel_times": (ip, [vp, dp, C.POINTER(ip)]),
             "cfd_reset_kernel_times": (ip, [vp]),
@@ -141,6 +154,10 @@ def lib() -> C.CDLL:
             "cfd_write_state": (ip, [cfgp, dp, C.c_char_p, C.c_double]),
             "cfd_write_schlieren": (ip, [cfgp, dp, C.c_char_p, C.c_double]),
             "cfd_write_masschange": (ip, [cfgp, C.c_char_p, ip, dp, dp, dp]),
+            "cfd_write_lineout": (ip, [cfgp, dp, C.c_char_p, ip]),
+            "cfd_read_settings": (ip, [C.c_char_p, C.POINTER(Settings)]),
+            "cfd_settings_config": (ip, [C.POINTER(Settings), cfgp]),
+            "cfd_settings_ic": (ip, [C.POINTER(Settings), cfgp, dp]),
             "cfd_batch_create": (ip, [vp, C.c_size_t, C.POINTER(vp)]),
             "cfd_batch_destroy": (ip, [vp]),
             "cfd_batch_member_bytes": (ip, [cfgp, C.POINTER(C.c_size_t)]),
@@ -275,10 +292,13 @@ class Solver:
         check(lib().cfd_upload_case(self._h, test_case.encode(), seed, n, t),
               f"cfd_upload_case({test_case})")
 
+    def set_reference_ghosts(self, enable: bool = True) -> None:
+        check(lib().cfd_set_reference_ghosts(self._h, int(enable)), "cfd_set_reference_ghosts")
+
     def download(self, layout: int = GHOSTED_AOS, out: np.ndarray | None = None) -> np.ndarray:
         c = self.cfg
         if out is None:
-            shape = c.ghosted_shape() if layout == GHOSTED_AOS else (c.nvar, c.ny, c.nx)
+            shape = c.ghosted_shape() if layout != SOA else (c.nvar, c.ny, c.nx)
             out = np.empty(shape)
         check(lib().cfd_download(self._h, _dp(out), layout), "cfd_download")
         return out

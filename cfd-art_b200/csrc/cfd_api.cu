@@ -15,6 +15,7 @@
 
 #include "../../include/cfdgpu.h"
 #include "cfd_error.h"
+#include "cfd_frame.h"
 #include "cfd_ic.h"
 #include "cfd_sweep.cuh"
 #include "ic_builders.h"
@@ -73,6 +74,9 @@ struct cfd_solver {
     Eos eos;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
+    // reference ghost values (cfd_set_reference_ghosts): the ghost frame
+    double* frame = nullptr;
+    bool ref_ghosts = false;
     // kernel timing: event pairs around each sweep launch, by sweep direction
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[2];
@@ -223,10 +227,18 @@ int timed_sweep(cfd_solver* s, int dir, const SweepArgs& a, int blocks) {
 // y other -> cur, x/2 cur -> other, and the last sweep flips cur.  The
 // buffer roles are resolved on the device, so a step skipped because t >= T
 // leaves them untouched.
+int enqueue_frame_snapshot(cfd_solver* s, int in_sel, bool host_dt);
+
 int enqueue_step(cfd_solver* s, bool host_dt, double dt) {
     const cfd_config& c = s->cfg;
     int bx = sweep_blocks(c, DIR_X), by = sweep_blocks(c, DIR_Y);
     int r;
+    // reference ghost values: the buffer current after the step keeps the
+    // fill made before the sweep that read it last (naive: the x sweep;
+    // Strang: the y sweep)
+    if (s->ref_ghosts &&
+        (r = enqueue_frame_snapshot(s, c.splitting == CFD_SPLIT_NAIVE ? 0 : 1, host_dt)))
+        return r;
     if (c.splitting == CFD_SPLIT_NAIVE) {
         SweepArgs ax = sweep_args(s, DIR_X, 0, 1.0, host_dt, dt, false, false);
         if ((r = timed_sweep(s, DIR_X, ax, bx))) return r;
@@ -281,6 +293,86 @@ __global__ void soa_to_ghosted(const double* __restrict__ src, double* __restric
             d[k] = (k == neg) ? -v : v;
         }
     }
+}
+
+// ---- reference ghost values --------------------------------------------------
+// The reference's grid keeps its ghost cells between boundary fills: after
+// set_ICs they hold the initial condition's own values, later the fill that
+// pre_sweep (E/sourcecode/euler_ppsweep.cpp:7-118) made before the last sweep
+// that read the buffer, and the corners are never refilled.  The solver keeps
+// those values in a ghost frame (cfd_frame.h) when asked to.
+
+// Every ghost cell (corners included) of a ghosted AoS grid.
+__global__ void frame_from_ghosted(const double* __restrict__ src, double* __restrict__ frame,
+                                   int nx, int ny, int g, int nv) {
+    const long long n = frame_cells(nx, ny, g);
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < n;
+         f += (long long)gridDim.x * blockDim.x) {
+        int gi, gj;
+        frame_cell(f, nx, ny, g, gi, gj);
+        const double* c = src + ((long long)gi * (nx + 2 * g) + gj) * nv;
+        for (int k = 0; k < nv; ++k) frame[f * nv + k] = c[k];
+    }
+}
+
+// The boundary fill of the sweep input bufs[cur ^ in_sel] into the frame's
+// edge cells (corners untouched), skipped like the sweeps once the device
+// time loop is done.
+__global__ void frame_snapshot(const double* __restrict__ b0, const double* __restrict__ b1, int in_sel, const DevState* st,
+                               int use_host_dt, double* __restrict__ frame, int nx, int ny, int g,
+                               int nv, int pitch, long long plane, int bcL, int bcR, int bcB,
+                               int bcT, int im, int it) {
+    if (!use_host_dt && st->done) return;
+    const double* __restrict__ src = ((st->cur ^ in_sel) & 1) ? b1 : b0;
+    const long long n = frame_cells(nx, ny, g);
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < n;
+         f += (long long)gridDim.x * blockDim.x) {
+        int gi, gj;
+        frame_cell(f, nx, ny, g, gi, gj);
+        const int i = gi - g, j = gj - g;
+        const bool ri = i >= 0 && i < ny, rj = j >= 0 && j < nx;
+        if (!ri && !rj) continue;  // corner
+        int si = i, sj = j, neg = -1;
+        if (j < 0) { sj = -j - 1; if (bcL) neg = im; }
+        else if (j >= nx) { sj = 2 * nx - 1 - j; if (bcR) neg = im; }
+        if (i < 0) { si = -i - 1; if (bcB) neg = it; }
+        else if (i >= ny) { si = 2 * ny - 1 - i; if (bcT) neg = it; }
+        for (int k = 0; k < nv; ++k) {
+            double v = src[k * plane + (long long)si * pitch + sj];
+            frame[f * nv + k] = (k == neg) ? -v : v;
+        }
+    }
+}
+
+// Interior from the SoA state, ghost cells from the frame.
+__global__ void soa_frame_to_ghosted(const double* __restrict__ src,
+                                     const double* __restrict__ frame, double* __restrict__ dst,
+                                     int nx, int ny, int g, int nv, int pitch, long long plane) {
+    int W = nx + 2 * g, H = ny + 2 * g;
+    long long n = (long long)W * H;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int gi = (int)(idx / W), gj = (int)(idx % W);
+        int i = gi - g, j = gj - g;
+        double* d = dst + idx * nv;
+        if (i >= 0 && i < ny && j >= 0 && j < nx) {
+            for (int k = 0; k < nv; ++k) d[k] = src[k * plane + (long long)i * pitch + j];
+        } else {
+            const double* fr = frame + frame_index(gi, gj, nx, ny, g) * nv;
+            for (int k = 0; k < nv; ++k) d[k] = fr[k];
+        }
+    }
+}
+
+int enqueue_frame_snapshot(cfd_solver* s, int in_sel, bool host_dt) {
+    const cfd_config& c = s->cfg;
+    int im = c.model == CFD_MODEL_EULER ? 1 : 2;
+    frame_snapshot<<<148, 256, 0, s->stream>>>(
+        s->buf[0], s->buf[1], in_sel, s->dst, host_dt ? 1 : 0, s->frame, c.nx, c.ny, s->g, s->nv,
+        s->pitch, s->plane, c.bc[CFD_BC_LEFT], c.bc[CFD_BC_RIGHT], c.bc[CFD_BC_BOTTOM],
+        c.bc[CFD_BC_TOP], im, im + 1);
+    CUDA_TRY(cudaGetLastError());
+    return CFD_OK;
 }
 
 template <int MODEL>
@@ -535,6 +627,7 @@ int cfd_destroy(cfd_solver* s) {
     cudaFree(s->dst);
     cudaFree(s->partials);
     cudaFree(s->counters);
+    cudaFree(s->frame);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return CFD_OK;
@@ -554,6 +647,15 @@ static int set_time(cfd_solver* s, int n, double t) {
     return CFD_OK;
 }
 
+// Ghost frame of a state uploaded without ghost values: the boundary fill of
+// the current state, corners zero.
+static int frame_from_state(cfd_solver* s) {
+    const cfd_config& c = s->cfg;
+    CUDA_TRY(cudaMemsetAsync(s->frame, 0,
+                             sizeof(double) * s->nv * frame_cells(c.nx, c.ny, s->g), s->stream));
+    return enqueue_frame_snapshot(s, 0, true);
+}
+
 int cfd_upload(cfd_solver* s, const double* host, int layout, int n, double t) {
     if (!s || !host) return fail(CFD_ERR_INVALID, "null argument");
     const cfd_config& c = s->cfg;
@@ -565,6 +667,11 @@ int cfd_upload(cfd_solver* s, const double* host, int layout, int n, double t) {
         ghosted_to_soa<<<148 * 8, 256, 0, s->stream>>>(s->buf[1], s->buf[0], c.nx, c.ny, s->g,
                                                        s->nv, s->pitch, s->plane);
         CUDA_TRY(cudaGetLastError());
+        if (s->frame) {
+            frame_from_ghosted<<<148, 256, 0, s->stream>>>(s->buf[1], s->frame, c.nx, c.ny, s->g,
+                                                           s->nv);
+            CUDA_TRY(cudaGetLastError());
+        }
     } else if (layout == CFD_LAYOUT_SOA) {
         for (int k = 0; k < s->nv; ++k)
             CUDA_TRY(cudaMemcpy2DAsync(s->buf[0] + k * s->plane, s->pitch * sizeof(double),
@@ -575,6 +682,7 @@ int cfd_upload(cfd_solver* s, const double* host, int layout, int n, double t) {
         return fail(CFD_ERR_INVALID, "unknown layout %d", layout);
     }
     if ((r = set_time(s, n, t))) return r;
+    if (s->frame && layout != CFD_LAYOUT_GHOSTED_AOS && (r = frame_from_state(s))) return r;
     if ((r = enqueue_reduce(s))) return r;
     s->uploaded = true;
     return CFD_OK;
@@ -590,6 +698,7 @@ int cfd_upload_device(cfd_solver* s, const double* dev, int n, double t) {
                                    s->stream));
     int r;
     if ((r = set_time(s, n, t))) return r;
+    if (s->frame && (r = frame_from_state(s))) return r;
     if ((r = enqueue_reduce(s))) return r;
     s->uploaded = true;
     return CFD_OK;
@@ -603,6 +712,8 @@ static int upload_program(cfd_solver* s, const std::vector<cfdic::Op>& ops, cons
     cfdic::Geom geo{c.x0, c.y0, c.dx, c.dy};
     CUDA_TRY(cfdic::build_device(ops, q, geo, c.nx, c.ny, s->buf[0], s->plane, s->pitch,
                                  s->stream));
+    if (s->frame)
+        CUDA_TRY(cfdic::build_frame_device(ops, q, geo, c.nx, c.ny, s->g, s->frame, s->stream));
     int r;
     if ((r = set_time(s, n, t))) return r;
     if ((r = enqueue_reduce(s))) return r;
@@ -651,6 +762,15 @@ int cfd_download(cfd_solver* s, double* host, int layout) {
         soa_to_ghosted<<<148 * 8, 256, 0, s->stream>>>(
             src, scratch, c.nx, c.ny, s->g, s->nv, s->pitch, s->plane, c.bc[0], c.bc[1],
             c.bc[2], c.bc[3], im, im + 1);
+        CUDA_TRY(cudaGetLastError());
+        size_t elems = (size_t)s->nv * (c.nx + 2 * s->g) * (size_t)(c.ny + 2 * s->g);
+        CUDA_TRY(cudaMemcpyAsync(host, scratch, elems * sizeof(double), cudaMemcpyDeviceToHost,
+                                 s->stream));
+    } else if (layout == CFD_LAYOUT_GHOSTED_AOS_AS_REFERENCE) {
+        if (!s->frame)
+            return fail(CFD_ERR_STATE, "reference ghost values are off (cfd_set_reference_ghosts)");
+        soa_frame_to_ghosted<<<148 * 8, 256, 0, s->stream>>>(src, s->frame, scratch, c.nx, c.ny,
+                                                             s->g, s->nv, s->pitch, s->plane);
         CUDA_TRY(cudaGetLastError());
         size_t elems = (size_t)s->nv * (c.nx + 2 * s->g) * (size_t)(c.ny + 2 * s->g);
         CUDA_TRY(cudaMemcpyAsync(host, scratch, elems * sizeof(double), cudaMemcpyDeviceToHost,
@@ -740,6 +860,38 @@ int cfd_advance(cfd_solver* s, int max_steps) {
     }
     for (int i = 0; i < max_steps % K; ++i)
         if ((r = enqueue_step(s, false, 0.0))) return r;
+    return CFD_OK;
+}
+
+int cfd_set_reference_ghosts(cfd_solver* s, int enable) {
+    if (!s) return fail(CFD_ERR_INVALID, "null solver");
+    const cfd_config& c = s->cfg;
+    if (s->graph) {  // the captured steps change
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    if (!enable) {
+        if (s->frame) {
+            CUDA_TRY(cudaStreamSynchronize(s->stream));
+            cudaFree(s->frame);
+            s->frame = nullptr;
+        }
+        s->ref_ghosts = false;
+        return CFD_OK;
+    }
+    if (!s->frame) {
+        size_t bytes = sizeof(double) * s->nv * frame_cells(c.nx, c.ny, s->g);
+        cudaError_t e = cudaMalloc(&s->frame, bytes);
+        if (e != cudaSuccess) {
+            s->frame = nullptr;
+            return fail(CFD_ERR_NOMEM, "ghost frame: %s", cudaGetErrorString(e));
+        }
+        CUDA_TRY(cudaMemsetAsync(s->frame, 0, bytes, s->stream));
+        int r;
+        if (s->uploaded && (r = enqueue_frame_snapshot(s, 0, true))) return r;
+    }
+    s->ref_ghosts = true;
     return CFD_OK;
 }
 

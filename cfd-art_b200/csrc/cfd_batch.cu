@@ -523,13 +523,22 @@ static int add_member(cfd_batch* b, const cfd_config* cfg, const double* host_ic
     I.eos.gm1_1 = I.eos.g1 - 1.0;
     I.eos.gm1_2 = I.eos.g2 - 1.0;
     I.eos.gp1 = I.eos.g1 * I.eos.p1;
-    I.g1f = (float)I.eos.g1;
-    I.p1f = (float)I.eos.p1;
-    I.g2f = (float)I.eos.g2;
-    I.p2f = (float)I.eos.p2;
-    I.gm1_1f = (float)I.eos.gm1_1;
-    I.gm1_2f = (float)I.eos.gm1_2;
-    I.gp1f = (float)I.eos.gp1;
+    const double c1 = I.eos.g1 * I.eos.p1 / I.eos.gm1_1, c2 = I.eos.g2 * I.eos.p2 / I.eos.gm1_2;
+    I.pf[0] = (float)I.eos.g1;
+    I.pf[1] = (float)I.eos.p1;
+    I.pf[2] = (float)I.eos.gm1_1;
+    I.pf[3] = (float)I.eos.gp1;
+    I.pf[4] = (float)(1.0 / I.eos.gm1_1);
+    I.pf[5] = (float)(1.0 / I.eos.gm1_2);
+    I.pf[6] = (float)c1;
+    I.pf[7] = (float)c2;
+    I.pd[0] = 1.0 / I.eos.gm1_1;
+    I.pd[1] = 1.0 / I.eos.gm1_2;
+    I.pd[2] = c1;
+    I.pd[3] = c2;
+    const bool stiff = I.eos.p1 != 0.0 || (c.model == CFD_MODEL_ALLAIRE && I.eos.p2 != 0.0);
+    I.flags = (c.limiter & 3) | (c.wavespeed == CFD_WS_PVRS ? MF_PVRS : 0) |
+              (I.godunov ? MF_GODUNOV : 0) | (stiff ? MF_STIFF : 0);
     I.max_steps = max_steps;
     I.active = 1;
     // upload: the ghosted FP64 grid (or the device-built SoA state) goes

@@ -16,4 +16,10 @@ namespace cfdic {
 cudaError_t build_device(const std::vector<Op>& ops, const Eos& q, const Geom& G, int nx, int ny,
                          double* soa, long long plane, int pitch, cudaStream_t stream);
 
+// Evaluates `ops` for every ghost cell (corners included) of the grid with
+// g ghost layers, into a ghost frame (cfd_frame.h), as set_ICs fills the
+// reference's ghost cells.
+cudaError_t build_frame_device(const std::vector<Op>& ops, const Eos& q, const Geom& G, int nx,
+                               int ny, int g, double* frame, cudaStream_t stream);
+
 }  // namespace cfdic

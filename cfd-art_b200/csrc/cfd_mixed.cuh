@@ -40,7 +40,13 @@ struct Inst {
     double dx, dy;
     double z_min;
     Eos eos;         // FP64 material parameters
-    float g1f, p1f, g2f, p2f, gm1_1f, gm1_2f, gp1f;
+    // FP32 constants of the sweeps (loaded into registers once per tile):
+    // g1, p1, g1 - 1, g1 p1, 1/(g1 - 1), 1/(g2 - 1), g1 p1/(g1 - 1), g2 p2/(g2 - 1)
+    alignas(16) float pf[8];
+    int flags;       // limiter (bits 0-1), PVRS speeds (2), Godunov (3), stiffened gas (4)
+    // FP64 mixture constants for the pressure of stiffened-gas cells:
+    // 1/(g1 - 1), 1/(g2 - 1), g1 p1/(g1 - 1), g2 p2/(g2 - 1)
+    double pd[4];
     DevState* st;
     double* partials;   // 4 per y tile
     int tiles_x, tiles_y;   // tiles of each sweep
@@ -56,18 +62,40 @@ struct MixedArgs {
     int chunk;              // CTA c walks tiles [c * chunk, (c + 1) * chunk) (persistent)
 };
 
+// Per-tile constants held in registers (one vector load per tile instead of
+// a global load at every use).
+struct MPar {
+    float g1, p1, gm1, gp1, i1, i2, c1, c2;
+    int flags;
+    __device__ __forceinline__ int limiter() const { return flags & 3; }
+    __device__ __forceinline__ bool pvrs() const { return (flags >> 2) & 1; }
+    __device__ __forceinline__ bool godunov() const { return (flags >> 3) & 1; }
+    __device__ __forceinline__ bool stiff() const { return (flags >> 4) & 1; }
+};
+enum { MF_PVRS = 4, MF_GODUNOV = 8, MF_STIFF = 16 };
+
+__device__ __forceinline__ MPar load_par(const Inst& I) {
+    const float4 a = *reinterpret_cast<const float4*>(I.pf);
+    const float4 b = *reinterpret_cast<const float4*>(I.pf + 4);
+    MPar P;
+    P.g1 = a.x; P.p1 = a.y; P.gm1 = a.z; P.gp1 = a.w;
+    P.i1 = b.x; P.i2 = b.y; P.c1 = b.z; P.c2 = b.w;
+    P.flags = I.flags;
+    return P;
+}
+
 __device__ __forceinline__ float frcp(float x) { return 1.0f / x; }
 __device__ __forceinline__ float fdiv(float a, float b) { return a / b; }
 __device__ __forceinline__ float fsqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ float fminf_s(float a, float b) { return (b < a) ? b : a; }
 __device__ __forceinline__ float fmaxf_s(float a, float b) { return (a < b) ? b : a; }
 
-// Mixture coefficients eps(z), k(z) in FP32 and FP64.
-__device__ __forceinline__ void mix_f(const Inst& I, float z, float& eps, float& k) {
+// Mixture coefficients eps(z) = z/(g1-1) + (1-z)/(g2-1) and
+// k(z) = (z g1 p1/(g1-1) + (1-z) g2 p2/(g2-1)) / eps in FP32.
+__device__ __forceinline__ void mix_f(const MPar& P, float z, float& eps, float& k) {
     float omz = 1.0f - z;
-    eps = fdiv(z, I.gm1_1f) + fdiv(omz, I.gm1_2f);
-    float num = fdiv(z * I.g1f * I.p1f, I.gm1_1f) + fdiv(omz * I.g2f * I.p2f, I.gm1_2f);
-    k = fdiv(num, eps);
+    eps = z * P.i1 + omz * P.i2;
+    k = (z * P.c1 + omz * P.c2) * frcp(eps);
 }
 
 // Primitive state (rho-split for Allaire: W = rho1 z, rho2 (1-z), u, v, p, z).
@@ -78,15 +106,15 @@ template <int MODEL> struct PrimF {
 // Conserved (hi + lo) -> primitive.  The pressure of a stiffened gas comes
 // from the FP64 sum hi + lo.
 template <int MODEL>
-__device__ __forceinline__ void c2p_mixed(const Inst& I, const float* hi, const float* lo,
-                                          float* W) {
+__device__ __forceinline__ void c2p_mixed(const Inst& I, const MPar& P, const float* hi,
+                                          const float* lo, float* W) {
     if constexpr (MODEL == MODEL_EULER) {
         float rho = hi[0];
         float r = frcp(rho);
         float u = hi[1] * r, v = hi[2] * r;
         float p;
-        if (I.p1f == 0.0f) {
-            p = I.gm1_1f * (hi[3] - 0.5f * (hi[1] * u + hi[2] * v));
+        if (!P.stiff()) {
+            p = P.gm1 * (hi[3] - 0.5f * (hi[1] * u + hi[2] * v));
         } else {
             double R = (double)hi[0] + (double)lo[0];
             double M1 = (double)hi[1] + (double)lo[1], M2 = (double)hi[2] + (double)lo[2];
@@ -104,18 +132,20 @@ __device__ __forceinline__ void c2p_mixed(const Inst& I, const float* hi, const 
         float u = hi[2] * r, v = hi[3] * r;
         float z = hi[5];
         float p;
-        if (I.p1f == 0.0f && I.p2f == 0.0f) {
-            float eps, k;
-            mix_f(I, z, eps, k);
+        if (!P.stiff()) {
+            float eps = z * P.i1 + (1.0f - z) * P.i2;
             p = fdiv(hi[4] - 0.5f * (hi[2] * u + hi[3] * v), eps);
         } else {
+            // p = (rho e - kn) / eps with rho e = E - |M|^2 / (2 R) and
+            // kn = eps k, as one FP64 division: (E R - |M|^2/2 - kn R) / (R eps)
             double R = ((double)hi[0] + (double)lo[0]) + ((double)hi[1] + (double)lo[1]);
             double M1 = (double)hi[2] + (double)lo[2], M2 = (double)hi[3] + (double)lo[3];
             double E = (double)hi[4] + (double)lo[4];
             double zz = (double)hi[5] + (double)lo[5];
-            Mix m = mix_coeffs(I.eos, zz);
-            double re = E - 0.5 * (M1 * M1 + M2 * M2) / R;
-            p = (float)(re / m.eps - m.k);
+            double omz = 1.0 - zz;
+            double eps = zz * I.pd[0] + omz * I.pd[1];
+            double kn = zz * I.pd[2] + omz * I.pd[3];
+            p = (float)(((E * R - 0.5 * (M1 * M1 + M2 * M2)) - kn * R) / (R * eps));
         }
         W[0] = hi[0];
         W[1] = hi[1];
@@ -128,13 +158,15 @@ __device__ __forceinline__ void c2p_mixed(const Inst& I, const float* hi, const 
 
 // Physical primitive state: the conversion to conserved variables would give
 // rho >= 0 and e >= 0 (and 0 <= z <= 1, partial densities >= 0).
-template <int MODEL> __device__ __forceinline__ bool phys_prim(const Inst& I, const float* W) {
+template <int MODEL> __device__ __forceinline__ bool phys_prim(const MPar& P, const float* W) {
     if constexpr (MODEL == MODEL_EULER) {
-        return W[0] >= 0.0f && W[3] + I.gp1f >= 0.0f;
+        return W[0] >= 0.0f && W[3] + P.gp1 >= 0.0f;
     } else {
-        float eps, k;
-        mix_f(I, W[5], eps, k);
-        return W[0] >= 0.0f && W[1] >= 0.0f && W[5] >= 0.0f && W[5] <= 1.0f && W[4] + k >= 0.0f;
+        // p + k >= 0  <=>  p eps + kn >= 0 (eps > 0 for 0 <= z <= 1)
+        float omz = 1.0f - W[5];
+        float eps = W[5] * P.i1 + omz * P.i2, kn = W[5] * P.c1 + omz * P.c2;
+        return W[0] >= 0.0f && W[1] >= 0.0f && W[5] >= 0.0f && W[5] <= 1.0f &&
+               W[4] * eps + kn >= 0.0f;
     }
 }
 
@@ -154,22 +186,23 @@ __device__ __forceinline__ float limit_f(int lim, float a, float b) {
 }
 
 // Sound speed of a primitive state.
-template <int MODEL> __device__ __forceinline__ float sound_f(const Inst& I, const float* W) {
+template <int MODEL> __device__ __forceinline__ float sound_f(const MPar& P, const float* W) {
     if constexpr (MODEL == MODEL_EULER) {
-        return fsqrt(fmaxf_s(0.0f, fdiv(I.g1f * (W[3] + I.p1f), W[0])));
+        return fsqrt(fmaxf_s(0.0f, fdiv(P.g1 * (W[3] + P.p1), W[0])));
     } else {
-        float eps, k;
-        mix_f(I, W[5], eps, k);
+        // c^2 = (k + p (1/eps + 1)) / rho = (kn + p (1 + eps)) / (eps rho)
+        float omz = 1.0f - W[5];
+        float eps = W[5] * P.i1 + omz * P.i2, kn = W[5] * P.c1 + omz * P.c2;
         float rho = W[0] + W[1];
-        return fsqrt(fmaxf_s(0.0f, fdiv(k + W[4] * (frcp(eps) + 1.0f), rho)));
+        return fsqrt(fmaxf_s(0.0f, fdiv(kn + W[4] * (1.0f + eps), eps * rho)));
     }
 }
 
 // Half-step evolution X = (0.5 dt/dx) A(W) d (primitive Jacobian).
 template <int MODEL>
-__device__ __forceinline__ void jac_f(const Inst& I, const float* W, const float* d, float s,
+__device__ __forceinline__ void jac_f(const MPar& P, const float* W, const float* d, float s,
                                       float* X) {
-    float c = sound_f<MODEL>(I, W);
+    float c = sound_f<MODEL>(P, W);
     if constexpr (MODEL == MODEL_EULER) {
         float rho = W[0], u = W[1];
         X[0] = s * (u * d[0] + rho * d[1]);
@@ -191,7 +224,7 @@ __device__ __forceinline__ void jac_f(const Inst& I, const float* W, const float
 // states as hllc_flux in cfd_physics.cuh).  F[NV] = flux, F[NV] = u*,
 // F[NV+1] = z* (Allaire).
 template <int MODEL>
-__device__ __forceinline__ void hllc_prim(const Inst& I, const float* WL, const float* WR,
+__device__ __forceinline__ void hllc_prim(const MPar& P, const float* WL, const float* WR,
                                           float* F) {
     using T = ModelTraits<MODEL>;
     constexpr int NV = T::NV;
@@ -199,18 +232,18 @@ __device__ __forceinline__ void hllc_prim(const Inst& I, const float* WL, const 
     if constexpr (MODEL == MODEL_EULER) {
         rL = WL[0]; uL = WL[1]; pL = WL[3];
         rR = WR[0]; uR = WR[1]; pR = WR[3];
-        cL = fsqrt(fmaxf_s(0.0f, fdiv(I.g1f * (pL + I.p1f), rL)));
-        cR = fsqrt(fmaxf_s(0.0f, fdiv(I.g1f * (pR + I.p1f), rR)));
+        cL = fsqrt(fmaxf_s(0.0f, fdiv(P.g1 * (pL + P.p1), rL)));
+        cR = fsqrt(fmaxf_s(0.0f, fdiv(P.g1 * (pR + P.p1), rR)));
     } else {
         rL = WL[0] + WL[1]; uL = WL[2]; pL = WL[4];
         rR = WR[0] + WR[1]; uR = WR[2]; pR = WR[4];
-        mix_f(I, WL[5], epsL, kL);
-        mix_f(I, WR[5], epsR, kR);
+        mix_f(P, WL[5], epsL, kL);
+        mix_f(P, WR[5], epsR, kR);
         cL = fsqrt(fmaxf_s(0.0f, fdiv(kL + pL * (frcp(epsL) + 1.0f), rL)));
         cR = fsqrt(fmaxf_s(0.0f, fdiv(kR + pR * (frcp(epsR) + 1.0f), rR)));
     }
     float SL, SR;
-    if (MODEL == MODEL_ALLAIRE && I.wavespeed == WS_PVRS) {
+    if (MODEL == MODEL_ALLAIRE && P.pvrs()) {
         float ra = 0.5f * (rL + rR), ca = 0.5f * (cL + cR);
         float ppv = fmaxf_s(0.0f, 0.5f * (pL + pR) + 0.5f * (uL - uR) * ra * ca);
         if (ppv > pL) {
@@ -245,7 +278,7 @@ __device__ __forceinline__ void hllc_prim(const Inst& I, const float* WL, const 
         U[0] = rho;
         U[1] = rho * u;
         U[2] = rho * v;
-        U[3] = fdiv(p + I.gp1f, I.gm1_1f) + 0.5f * rho * (u * u + v * v);
+        U[3] = (p + P.gp1) * P.i1 + 0.5f * rho * (u * u + v * v);
     } else {
         float v = W[3];
         float eps = left ? epsL : epsR, k = left ? kL : kR;
@@ -404,10 +437,16 @@ __device__ __forceinline__ void tile_fetch(const MixedArgs& A, const TileGeom& g
     load_cell<MODEL>(I, g.cur ^ (DIR == DIR_Y), off, h, l);
 }
 
+// Per-thread wave-speed maxima and mass sums of the tiles of a run.
+struct RAcc {
+    float mu, mv;
+    double m1, m2;
+};
+
 template <int MODEL, int DIR, int TS, int NA>
 __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g, float* h,
                                            float* l, bool& neg, int next_tile, char* smem,
-                                           double* racc) {
+                                           RAcc& racc) {
     using Tl = MTile<MODEL, DIR, TS, NA>;
     using MT = ModelTraits<MODEL>;
     constexpr int NV = MT::NV, LA = Tl::LA, NSLOT = Tl::NSLOT, ST = Tl::ST;
@@ -423,6 +462,7 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
     unsigned char* sFl = reinterpret_cast<unsigned char*>(smem + 6 * Tl::VB * NSLOT + 8 * NSLOT);
 
     const Inst& I = A.insts[g.inst];
+    const MPar P = load_par(I);
     DevState* st = I.st;
     const double dt = st->dt;
     const double h_flux = (DIR == DIR_X) ? I.dx : (I.fix_dy ? I.dy : I.dx);
@@ -444,7 +484,7 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
         }
         int s = Tl::slot(a, b);
         float W[NV];
-        c2p_mixed<MODEL>(I, h, l, W);
+        c2p_mixed<MODEL>(I, P, h, l, W);
         sH.put(s, h);
         sL.put(s, l);
         sW.put(s, W);
@@ -457,7 +497,7 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
     __syncthreads();
 
     // ---- P2: slopes and evolved face states (primitive) ----------------
-    if (!I.godunov && tid < (LA - 2) * NA) {
+    if (!P.godunov() && tid < (LA - 2) * NA) {
         int a, b;
         Tl::item(tid, 1, LA - 2, a, b);
         int s = Tl::slot(a, b);
@@ -466,22 +506,22 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
         sW.get(s - ST, Wl);
         sW.get(s + ST, Wr);
 #pragma unroll
-        for (int k = 0; k < NV; ++k) d[k] = limit_f(I.limiter, W[k] - Wl[k], Wr[k] - W[k]);
+        for (int k = 0; k < NV; ++k) d[k] = limit_f(P.limiter(), W[k] - Wl[k], Wr[k] - W[k]);
         unsigned fl = 0;
 #pragma unroll
         for (int k = 0; k < NV; ++k) Wt[k] = W[k] + 0.5f * d[k];
-        if (phys_prim<MODEL>(I, Wt)) fl |= 1u;
+        if (phys_prim<MODEL>(P, Wt)) fl |= 1u;
 #pragma unroll
         for (int k = 0; k < NV; ++k) Wt[k] = W[k] - 0.5f * d[k];
-        if (phys_prim<MODEL>(I, Wt)) fl |= 2u;
-        jac_f<MODEL>(I, W, d, s_half, X);
+        if (phys_prim<MODEL>(P, Wt)) fl |= 2u;
+        jac_f<MODEL>(P, W, d, s_half, X);
 #pragma unroll
         for (int k = 0; k < NV; ++k) Wt[k] = (W[k] + 0.5f * d[k]) - X[k];
-        if (phys_prim<MODEL>(I, Wt)) fl |= 4u;
+        if (phys_prim<MODEL>(P, Wt)) fl |= 4u;
         sP.put(s, Wt);
 #pragma unroll
         for (int k = 0; k < NV; ++k) Wt[k] = (W[k] - 0.5f * d[k]) - X[k];
-        if (phys_prim<MODEL>(I, Wt)) fl |= 8u;
+        if (phys_prim<MODEL>(P, Wt)) fl |= 8u;
         sM.put(s, Wt);
         sFl[s] = (unsigned char)fl;
     }
@@ -494,7 +534,7 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
         int sR = Tl::slot(a, b), sL = sR - ST;
         float WL[NV], WR[NV];
         bool first = true;
-        if (!I.godunov) {
+        if (!P.godunov()) {
             unsigned fL = sFl[sL], fR = sFl[sR];
             // zero slopes evolve to the cell state itself; the first-order
             // fallback uses the cell states too
@@ -509,14 +549,15 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
             sW.get(sR, WR);
         }
         float F[NV + 2];
-        hllc_prim<MODEL>(I, WL, WR, F);
+        hllc_prim<MODEL>(P, WL, WR, F);
         sF.put(sR, F);
         sUZ[sR] = make_float2(F[NV], MODEL == MODEL_ALLAIRE ? F[NV + 1] : 0.0f);
     }
     __syncthreads();
 
     // ---- P4: compensated update, store, reduce -----------------------------
-    double r_mu = 0.0, r_mv = 0.0, r_m1 = 0.0, r_m2 = 0.0;
+    float r_mu = 0.0f, r_mv = 0.0f;
+    double r_m1 = 0.0, r_m2 = 0.0;
     if (tid < TS * NA) {
         int a, b;
         Tl::item(tid, 2, TS, a, b);
@@ -544,7 +585,7 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
                 float usL = uzL.x, usR = uzR.x, zsL = uzL.y, zsR = uzR.y;
                 float z = hh[5];
                 float dz;
-                if (I.godunov) {
+                if (P.godunov()) {
                     float zL = sH.v2[s - ST].y, zR = sH.v2[s + ST].y;
                     dz = -k_upd * ((zR - z) * fminf_s(0.0f, usR) + (z - zL) * fmaxf_s(0.0f, usL));
                 } else {
@@ -566,19 +607,19 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
                 oh[MT::IT] = t2; ol[MT::IT] = t2l;
             }
             float Wn[NV];
-            c2p_mixed<MODEL>(I, hh, ll, Wn);
+            c2p_mixed<MODEL>(I, P, hh, ll, Wn);
             if constexpr (MODEL == MODEL_EULER) {
                 // density / energy restore as in the plain form (rare)
-                if (!(hh[0] > 1e-12f) || !(Wn[3] + I.gp1f > 0.0f)) {
+                if (!(hh[0] > 1e-12f) || !(Wn[3] + P.gp1 > 0.0f)) {
                     float Wo[NV];
-                    c2p_mixed<MODEL>(I, oh, ol, Wo);
+                    c2p_mixed<MODEL>(I, P, oh, ol, Wo);
                     float rho = hh[0] > 1e-12f ? hh[0] : oh[0];
                     float u = Wn[1], v = Wn[2];
-                    float p = (Wn[3] + I.gp1f > 0.0f) ? Wn[3] : Wo[3];
+                    float p = (Wn[3] + P.gp1 > 0.0f) ? Wn[3] : Wo[3];
                     hh[0] = rho; ll[0] = 0.f;
                     hh[1] = rho * u; ll[1] = 0.f;
                     hh[2] = rho * v; ll[2] = 0.f;
-                    hh[3] = fdiv(p + I.gp1f, I.gm1_1f) + 0.5f * rho * (u * u + v * v); ll[3] = 0.f;
+                    hh[3] = (p + P.gp1) * P.i1 + 0.5f * rho * (u * u + v * v); ll[3] = 0.f;
                     Wn[0] = rho;
                     Wn[3] = p;
                 }
@@ -586,19 +627,19 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
             long long off = (DIR == DIR_X) ? (long long)gb * I.pitch + ga : (long long)ga * I.pitch + gb;
             store_cell<MODEL>(I, g.cur ^ (DIR == DIR_X), off, hh, ll);
             if (DIR == DIR_Y) {
-                float c = sound_f<MODEL>(I, Wn);
-                r_mu = (double)(fabsf(Wn[MT::IM]) + c);
-                r_mv = (double)(fabsf(Wn[MT::IT]) + c);
+                float c = sound_f<MODEL>(P, Wn);
+                r_mu = fabsf(Wn[MT::IM]) + c;
+                r_mv = fabsf(Wn[MT::IT]) + c;
                 r_m1 = (double)hh[0] + (double)ll[0];
                 if constexpr (MODEL == MODEL_ALLAIRE) r_m2 = (double)hh[1] + (double)ll[1];
             }
         }
     }
     if constexpr (DIR == DIR_Y) {  // this thread's wave speeds and masses
-        racc[0] = smax(racc[0], r_mu);
-        racc[1] = smax(racc[1], r_mv);
-        racc[2] += r_m1;
-        racc[3] += r_m2;
+        racc.mu = fmaxf_s(racc.mu, r_mu);  // max of FP32 speeds: exact in FP32
+        racc.mv = fmaxf_s(racc.mv, r_mv);
+        racc.m1 += r_m1;
+        racc.m2 += r_m2;
     }
 }
 
@@ -610,13 +651,13 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
 // in at most one run, and the CTAs that do are c0 = t0 / chunk ..
 // (t0 + n - 1) / chunk: slot c - c0 is written exactly once per sweep.
 __device__ __forceinline__ void flush_run(const MixedArgs& A, int inst, int slot, int nslots,
-                                          int count, double* racc, double dt) {
+                                          int count, RAcc& racc, double dt) {
     const Inst& I = A.insts[inst];
     DevState* st = I.st;
     __shared__ double red[4][8];
     __shared__ bool is_last;
     const int tid = threadIdx.x;
-    double mu = racc[0], mv = racc[1], m1 = racc[2], m2 = racc[3];
+    double mu = (double)racc.mu, mv = (double)racc.mv, m1 = racc.m1, m2 = racc.m2;
     for (int o = 16; o > 0; o >>= 1) {
         mu = smax(mu, __shfl_down_sync(0xffffffffu, mu, o));
         mv = smax(mv, __shfl_down_sync(0xffffffffu, mv, o));
@@ -652,7 +693,8 @@ __device__ __forceinline__ void flush_run(const MixedArgs& A, int inst, int slot
         __threadfence();
         finish_reduction(st, I.partials, nslots, 1, dt, 0);
     }
-    racc[0] = racc[1] = racc[2] = racc[3] = 0.0;
+    racc.mu = racc.mv = 0.0f;
+    racc.m1 = racc.m2 = 0.0;
 }
 
 // Persistent sweep: a fixed grid of CTAs walks the tile list of every
@@ -669,7 +711,7 @@ __global__ void __launch_bounds__(256, MODEL == MODEL_EULER ? 4 : 3) mixed_sweep
     if (t_begin >= t_end) return;
     TileGeom g = tile_geom<DIR, TS, NA>(A, t_begin);
     if (!g.skip) tile_fetch<MODEL, DIR, TS, NA>(A, g, h, l, neg);
-    double racc[4] = {0.0, 0.0, 0.0, 0.0};
+    RAcc racc{0.0f, 0.0f, 0.0, 0.0};
     int run_first = t_begin, run_count = 0;
     for (int tile = t_begin; tile < t_end; ++tile) {
         int next = tile + 1 < t_end ? tile + 1 : A.ntiles;  // A.ntiles: none

@@ -6,7 +6,10 @@
 // the initial condition with the restated set_ICs hooks, runs the time loop
 // of headers/simulation.hpp:48-61 with compute_dt and the split step on the
 // GPU, and writes the reference's gnuplot outputs with its cadence
-// (sourcecode/euler_io.cpp:1235-1261).
+// (sourcecode/euler_io.cpp:1235-1261, A/sourcecode/allaire_diffuse_io.cpp:1251-1294).
+// The solver keeps the reference's ghost values, so the outputs that read
+// ghost cells (schlieren at the domain edge, Allaire lineouts) are the
+// reference's too.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -39,6 +42,7 @@ int main(int argc, char** argv) {
     if ((rc = cfd_settings_ic(&sf, &cfg, grid.data()))) return die("initial condition", rc);
     cfd_solver* s = nullptr;
     if ((rc = cfd_create(&cfg, &s))) return die("cfd_create", rc);
+    if ((rc = cfd_set_reference_ghosts(s, 1))) return die("cfd_set_reference_ghosts", rc);
     if ((rc = cfd_upload(s, grid.data(), CFD_LAYOUT_GHOSTED_AOS, 0, 0.0))) return die("upload", rc);
 
     const std::string base = sf.basename;
@@ -46,15 +50,34 @@ int main(int argc, char** argv) {
     const double outputinterval = T / sf.output_freq;
     double lastoutputtime = 0.0;
     std::vector<double> tt, m1, m2;
+    const bool allaire = cfg.model == CFD_MODEL_ALLAIRE;
+    // A/sourcecode/allaire_diffuse_io.cpp:1259: extra schlieren frames
+    std::vector<double> schlieren_times;
+    if (allaire)
+        schlieren_times = {0.000115, 0.000175, 0.000247, 0.000307, 0.000378, 0.000402, 0.000477,
+                           0.001080};
+    bool have = false;  // grid holds the state of this output call
+    auto fetch = [&]() -> int {
+        if (have) return 0;
+        have = true;
+        return cfd_download(s, grid.data(), CFD_LAYOUT_GHOSTED_AOS_AS_REFERENCE);
+    };
     auto output = [&](int n, double t) -> int {
+        have = false;
+        int r;
+        if (!schlieren_times.empty() && t > schlieren_times[0]) {
+            if ((r = fetch())) return r;
+            cfd_write_schlieren(&cfg, grid.data(), base.c_str(), t);
+            schlieren_times.erase(schlieren_times.begin());
+        }
         bool final_out = (t == T);
         bool due = (n == 0 || final_out) ||
                    (sf.output_freq != 0 && t - lastoutputtime > outputinterval);
         if (!due) return 0;
-        int r = cfd_download(s, grid.data(), CFD_LAYOUT_GHOSTED_AOS);
-        if (r) return r;
+        if ((r = fetch())) return r;
         cfd_write_state(&cfg, grid.data(), base.c_str(), t);
         cfd_write_schlieren(&cfg, grid.data(), base.c_str(), t);
+        if (allaire && (n == 0 || final_out)) cfd_write_lineout(&cfg, grid.data(), base.c_str(), n);
         if (final_out && !tt.empty())
             cfd_write_masschange(&cfg, base.c_str(), (int)tt.size(), tt.data(), m1.data(), m2.data());
         if (!(n == 0 || final_out)) lastoutputtime = t;

@@ -214,6 +214,34 @@ int cfd_write_schlieren(const cfd_config* c, const double* grid, const char* bas
     return CFD_OK;
 }
 
+// A/sourcecode/allaire_diffuse_io.cpp:1188-1232: row Ny/2 and column Nx/2
+// of the ghosted grid (ghost cells included), -lineoutx-<n>.dat and
+// -lineouty-<n>.dat.
+int cfd_write_lineout(const cfd_config* c, const double* grid, const char* basename, int n) {
+    if (!c || !grid || !basename || c->model != CFD_MODEL_ALLAIRE) return CFD_ERR_INVALID;
+    View v = view_of(c, grid);
+    auto line = [&](std::ofstream& out, double coord, const double* U) {
+        double rho = U[0] + U[1];
+        double u = U[2] / rho;
+        double vv = U[3] / rho;
+        double e = U[4] / rho - 0.5 * (u * u + vv * vv);
+        double z = U[5];
+        double p = mixture_pressure(c, rho, e, z);
+        out << coord << " " << rho << " " << u << " " << vv << " " << e << " " << p << " " << z
+            << std::endl;
+    };
+    std::ofstream ox(std::string(basename) + "-lineoutx-" + std::to_string(n) + ".dat");
+    if (!ox) return CFD_ERR_INVALID;
+    int i = v.ny / 2;
+    for (int j = 0; j < v.nx + 2 * v.g; ++j) line(ox, v.ccx(j), v.cell(i, j));
+    ox.close();
+    std::ofstream oy(std::string(basename) + "-lineouty-" + std::to_string(n) + ".dat");
+    if (!oy) return CFD_ERR_INVALID;
+    int j = v.nx / 2;
+    for (int r = 0; r < v.ny + 2 * v.g; ++r) line(oy, v.ccy(r), v.cell(r, j));
+    return CFD_OK;
+}
+
 int cfd_write_masschange(const cfd_config* c, const char* basename, int nrec, const double* t,
                          const double* m1, const double* m2) {
     if (!c || !basename || nrec < 1 || !t || !m1) return CFD_ERR_INVALID;

@@ -42,7 +42,9 @@ enum { CFD_LIM_MINMOD = 0, CFD_LIM_VANLEER = 1, CFD_LIM_MC = 2, CFD_LIM_UNLIMITE
 enum { CFD_FLUX_MUSCL = 0, CFD_FLUX_GODUNOV = 1 };
 enum { CFD_SPLIT_NAIVE = 0, CFD_SPLIT_STRANG = 1 };
 enum { CFD_WS_DAVIS = 0, CFD_WS_PVRS = 1 };
-enum { CFD_LAYOUT_GHOSTED_AOS = 0, CFD_LAYOUT_SOA = 1 };
+/* CFD_LAYOUT_GHOSTED_AOS_AS_REFERENCE: cfd_download only, ghost cells as the
+ * reference's grid holds them at the same point (see cfd_set_reference_ghosts). */
+enum { CFD_LAYOUT_GHOSTED_AOS = 0, CFD_LAYOUT_SOA = 1, CFD_LAYOUT_GHOSTED_AOS_AS_REFERENCE = 2 };
 enum { CFD_BC_LEFT = 0, CFD_BC_RIGHT = 1, CFD_BC_BOTTOM = 2, CFD_BC_TOP = 3 };
 
 /* Event counters (cfd_status.counters); the reference prints or asserts. */
@@ -131,6 +133,19 @@ int cfd_upload_case(cfd_solver* s, const char* test_case, uint64_t seed, int n, 
 /* Copies the current state to the host in `layout`.  In the ghosted layout
  * the ghost strips hold the boundary fill of the current state. */
 int cfd_download(cfd_solver* s, double* host, int layout);
+
+/* Keeps the ghost values the reference's grid holds between boundary fills,
+ * for output writers that read ghost cells (the schlieren stencil at the
+ * domain edge, the Allaire lineouts): after an upload, the uploaded grid's
+ * own ghosts (the initial condition evaluated there, for the device
+ * builders; the boundary fill for the SoA layouts); after a step, the fill
+ * pre_sweep (sourcecode/euler_ppsweep.cpp:7-118) made before the last sweep
+ * that read the buffer now current (naive splitting: the step's x sweep;
+ * Strang: its y sweep); corners keep their initial values, as
+ * set_boundary_conditions never writes them.  Each step then launches one
+ * small extra kernel.  cfd_download with CFD_LAYOUT_GHOSTED_AOS_AS_REFERENCE
+ * returns these ghosts.  Enable before the upload to keep its ghost values. */
+int cfd_set_reference_ghosts(cfd_solver* s, int enable);
 
 /* problem_base::compute_dt (sourcecode/euler_timestep.cpp:7-44): dt for step
  * n at time t from the current state.  Synchronises the solver's stream. */

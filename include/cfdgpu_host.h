@@ -81,6 +81,10 @@ int cfd_settings_ic(const cfd_settings* s, const cfd_config* cfg, double* grid);
  * with <t> formatted like std::to_string(double). */
 int cfd_write_state(const cfd_config* cfg, const double* grid, const char* basename, double t);
 int cfd_write_schlieren(const cfd_config* cfg, const double* grid, const char* basename, double t);
+/* Allaire lineouts <basename>-lineoutx-<n>.dat and -lineouty-<n>.dat: row
+ * Ny/2 and column Nx/2 of the ghosted grid, ghost cells included
+ * (A/sourcecode/allaire_diffuse_io.cpp:1188-1232). */
+int cfd_write_lineout(const cfd_config* cfg, const double* grid, const char* basename, int n);
 /* <basename>-masschange.dat from per-step (t, mass1, mass2) records
  * (E: :1219-1233, A: :1235-1249). */
 int cfd_write_masschange(const cfd_config* cfg, const char* basename, int nrec, const double* t,

@@ -170,6 +170,17 @@ def ref_write(model: str, p: RefParams, grid: np.ndarray, basename: str, n: int,
     getattr(lib, f"ref_{model}_write")(C.byref(p), _dptr(grid), basename.encode(), int(n), float(t))
 
 
+def ref_simulate(model: str, settings_path: str) -> int:
+    """The reference's main() on a settings file: runs simulation::run_simulation
+    and writes its output files.  Its output cadence keeps static state, so call
+    it once per process."""
+    lib = ref_lib(model)
+    f = getattr(lib, f"ref_{model}_simulate")
+    f.argtypes = [C.c_char_p]
+    f.restype = C.c_int
+    return f(str(settings_path).encode())
+
+
 # --------------------------------------------------------------------------
 # plain-C restatement (cfd_oracle.c)
 

@@ -43,6 +43,8 @@
 #include "misc.hpp"
 #include "zupdate.hpp"
 #include "splitting_scheme.hpp"
+#include "settings_file.hpp"
+#include "simulation.hpp"
 #undef private
 #undef protected
 
@@ -366,7 +368,7 @@ int ref_allaire_case_ic(const char* test_case, int nx, int ny, const char* flux_
     return 0;
 }
 
-// Reference gnuplot writers (sourcecode/allaire_diffuse_io.cpp:1109-1186).
+// Reference gnuplot writers (sourcecode/allaire_diffuse_io.cpp:1109-1232).
 int ref_allaire_write(const ref_params* p, const double* grid, const char* basename, int n,
                       double t) {
     sim_info s = make_params(p);
@@ -380,8 +382,22 @@ int ref_allaire_write(const ref_params* p, const double* grid, const char* basen
     std::cout.rdbuf(sink.rdbuf());
     a.gnuplot_output(G, s, n, t);
     a.gnuplot_schlieren(G, s, n, t);
+    a.gnuplot_lineout(G, s, n, t);
     std::cout.rdbuf(old);
     return 0;
+}
+
+// HOOK: the reference's main() (sourcecode/main.cpp:17-49, with the allaire_diffuse problem its commented line 36 names):
+// reads a settings file and runs simulation::run_simulation, which writes
+// every output file with the reference's own cadence and writers.  Output
+// state is static inside the reference (last output time), so run it once
+// per process.
+int ref_allaire_simulate(const char* settings_path) {
+    settings_file sf;
+    sf.read_settings_file(settings_path);
+    std::shared_ptr<problem_base> problem = std::make_shared<allaire_diffuse>();
+    simulation sim(sf, problem);
+    return sim.run_simulation();
 }
 
 }  // extern "C"

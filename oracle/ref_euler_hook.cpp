@@ -44,6 +44,8 @@
 #include "riemann_solver_HLLC.hpp"
 #include "misc_euler.hpp"
 #include "splitting_scheme.hpp"
+#include "settings_file.hpp"
+#include "simulation.hpp"
 #undef private
 #undef protected
 
@@ -342,6 +344,19 @@ int ref_euler_write(const ref_params* p, const double* grid, const char* basenam
     e.gnuplot_schlieren(G, s, n, t);
     std::cout.rdbuf(old);
     return 0;
+}
+
+// HOOK: the reference's main() (sourcecode/main.cpp:17-49):
+// reads a settings file and runs simulation::run_simulation, which writes
+// every output file with the reference's own cadence and writers.  Output
+// state is static inside the reference (last output time), so run it once
+// per process.
+int ref_euler_simulate(const char* settings_path) {
+    settings_file sf;
+    sf.read_settings_file(settings_path);
+    std::shared_ptr<problem_base> problem = std::make_shared<Euler>();
+    simulation sim(sf, problem);
+    return sim.run_simulation();
 }
 
 }  // extern "C"

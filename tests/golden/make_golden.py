@@ -1,6 +1,7 @@
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # everything
+    python tests/golden/make_golden.py outputs    # only the whole-run output files
 
 Requires oracle/_ref/libref_{euler,allaire}.so (built by `make -C oracle ref`
 from the reference sources) and cfd-art_b200/lib/libcfdgpu.so (only for the
@@ -138,6 +139,46 @@ def main():
     kat_faces("euler", 256, 1)
     kat_faces("allaire", 256, 2)
 
+    for name, model, settings in OUTPUT_RUNS:
+        output_run(name, model, settings)
+
+
+# Whole runs of the reference's main() on a settings file: every output file
+# it writes (states, schlieren frames, lineouts, mass change), byte for byte.
+OUTPUT_RUNS = [
+    ("outputs_euler_cross_20x16", "euler",
+     "Nx 20\nNy 16\nCFL 0.5\nsplitting_scheme naive_splitting\ntest_case cross\n"
+     "output_freq 3\noutputpath {out}\nflux_solver MUSCL\nriemann_solver HLLC\nproblem euler\n"),
+    ("outputs_allaire_shocked_helium_bubble_26x8", "allaire",
+     "Nx 26\nNy 8\nCFL 0.5\nsplitting_scheme strang_splitting\n"
+     "test_case shocked_helium_bubble\noutput_freq 2\noutputpath {out}\nflux_solver MUSCL\n"
+     "riemann_solver HLLC\nproblem allaire\n"),
+]
+
+
+def output_run(name: str, model: str, settings: str) -> None:
+    import os
+    import subprocess
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "out") + "/"
+        os.makedirs(out)
+        sf = os.path.join(d, "settingsfile.txt")
+        with open(sf, "w") as f:
+            f.write(settings.format(out=out))
+        code = (f"import sys; sys.path.insert(0, {str(ROOT / 'oracle')!r}); import oracle_py as O; "
+                f"sys.exit(O.ref_simulate({model!r}, {sf!r}))")
+        subprocess.run([sys.executable, "-c", code], check=True, stdout=subprocess.DEVNULL,
+                       env={**os.environ, "OMP_NUM_THREADS": "1"})
+        files = {fn: np.frombuffer(open(os.path.join(out, fn), "rb").read(), np.uint8)
+                 for fn in sorted(os.listdir(out))}
+    np.savez_compressed(HERE / f"{name}.npz", settings=np.array(settings), **files)
+    print(f"{name}: {len(files)} files")
+
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["outputs"]:
+        for run in OUTPUT_RUNS:
+            output_run(*run)
+    else:
+        main()

@@ -17,7 +17,7 @@ from cfdtest import (GOLDEN, config_from_params, density, ghost_grid, load_golde
 pytestmark = pytest.mark.gpu
 TOL_L1 = 1e-12  # relative L1 density error bound of the plain FP64 form
 
-FIXTURES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("kat_"))
+FIXTURES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("kat_", "outputs_")))
 
 
 @pytest.mark.parametrize("model", ["euler", "allaire"])

@@ -91,8 +91,44 @@ def test_settings_file_roundtrip(tmp_path):
                  "test_case totem_pole_3\noutput_freq 40\noutputpath ./out/\n"
                  "flux_solver MUSCL\nriemann_solver HLLC\nproblem euler\nunknown_key 3\n")
     L = G.lib()
-    buf = (C.c_char * 4096)()
-    assert L.cfd_read_settings(str(f).encode(), C.cast(buf, C.c_void_p)) == 0 if False else True
+    st = G.Settings()
+    assert L.cfd_read_settings(str(f).encode(), C.byref(st)) == 0
+    assert (st.Nx, st.Ny, st.CFL, st.output_freq) == (30, 61, 0.5, 40)
+    assert st.splitting_scheme == b"naive_splitting" and st.test_case == b"totem_pole_3"
+    assert st.flux_solver == b"MUSCL" and st.riemann_solver == b"HLLC" and st.problem == b"euler"
+    # basename as headers/settings_file.hpp:69 builds it
+    assert st.basename == b"./out/euler-totem_pole_3-MUSCL-30-61"
+    assert st.seed == 20261203 and st.nbubbles == 32 and st.steps == 0
+    cfg = G.Config()
+    assert L.cfd_settings_config(C.byref(st), C.byref(cfg)) == 0
+    ref = G.case_config(G.EULER, "totem_pole_3", 30, 61)
+    assert (cfg.model, cfg.nx, cfg.ny, cfg.dx, cfg.dy, cfg.T, list(cfg.bc)) == \
+        (ref.model, ref.nx, ref.ny, ref.dx, ref.dy, ref.T, list(ref.bc))
+    assert cfg.cfl == 0.5 and cfg.splitting == G.SPLIT["naive"]
+    grid = np.zeros(cfg.ghosted_shape())
+    assert L.cfd_settings_ic(C.byref(st), C.byref(cfg), grid.ctypes.data_as(C.POINTER(C.c_double))) == 0
+    assert np.array_equal(grid, G.case_ic(cfg, "totem_pole_3"))
+
+
+def test_settings_extensions(tmp_path):
+    f = tmp_path / "settingsfile.txt"
+    f.write_text("Nx 64\nNy 32\nCFL 0.6\nsplitting_scheme strang_splitting\n"
+                 "test_case water_shock_air_bubble\noutput_freq 0\noutputpath o/\n"
+                 "flux_solver MUSCL\nriemann_solver HLLC\nproblem allaire\nprecision mixed\n"
+                 "limiter vanleer\nwavespeed pvrs\nsteps 7\nalpha_clip 1e-5\nseed 5\n")
+    L = G.lib()
+    st = G.Settings()
+    assert L.cfd_read_settings(str(f).encode(), C.byref(st)) == 0
+    cfg = G.Config()
+    assert L.cfd_settings_config(C.byref(st), C.byref(cfg)) == 0
+    assert cfg.model == G.ALLAIRE and cfg.precision == G.MIXED
+    assert cfg.splitting == G.SPLIT["strang"] and cfg.limiter == G.LIMITERS["vanleer"]
+    assert cfg.wavespeed == G.WAVESPEED["pvrs"] and cfg.z_min == 1e-5 and st.steps == 7
+    grid = np.zeros(cfg.ghosted_shape())
+    assert L.cfd_settings_ic(C.byref(st), C.byref(cfg), grid.ctypes.data_as(C.POINTER(C.c_double))) == 0
+    assert np.array_equal(grid, G.recipe_ic(cfg, "water_shock_air_bubble", seed=5))
+    st.riemann_solver = b"Roe"
+    assert L.cfd_settings_config(C.byref(st), C.byref(cfg)) != 0
 
 
 def test_header_symbols_exported():
@@ -137,3 +173,9 @@ def test_output_writers_match_reference(tmp_path, model, case):
         b = tmp_path / f"ours-{kind}-0.012346.dat"
         assert a.exists() and b.exists()
         assert filecmp.cmp(a, b, shallow=False), kind
+    if model == "allaire":
+        assert L.cfd_write_lineout(C.byref(cfg), gp, str(tmp_path / "ours").encode(), 5) == 0
+        for kind in ("lineoutx", "lineouty"):
+            a, b = tmp_path / f"ref-{kind}-5.dat", tmp_path / f"ours-{kind}-5.dat"
+            assert a.exists() and b.exists()
+            assert filecmp.cmp(a, b, shallow=False), kind

@@ -11,7 +11,7 @@ import pytest
 import oracle_py as O
 from cfdtest import GOLDEN, density, ghost_grid, load_golden, params_from, rel_l1
 
-FIXTURES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("kat_"))
+FIXTURES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("kat_", "outputs_")))
 
 pytestmark = pytest.mark.skipif(not O.port_available(), reason="oracle/_build not built")
 
@@ -90,3 +90,44 @@ def test_port_compute_dt_matches_reference(model):
     for n in (0, 4, 5, 9):
         for t in (0.0, p.T - 1e-5):
             assert O.port_compute_dt(model, p, grid, n, t)[0] == O.ref_compute_dt(model, p, grid, n, t)
+
+
+OUTPUT_RUNS = sorted(p.stem for p in GOLDEN.glob("outputs_*.npz"))
+
+
+@pytest.mark.parametrize("run", OUTPUT_RUNS)
+def test_port_and_writers_reproduce_reference_final_outputs(tmp_path, run):
+    """The oracle run to T with the reference's buffer semantics (ghost cells
+    as its grid holds them), written by the library's host writers, gives the
+    reference's final output files byte for byte."""
+    import ctypes as C
+
+    import cfdgpu as G
+    from cfdtest import params_from_config
+
+    fx = load_golden(run)
+    sf = tmp_path / "settingsfile.txt"
+    sf.write_text(str(fx["settings"]).format(out=str(tmp_path) + "/"))
+    L = G.lib()
+    st = G.Settings()
+    assert L.cfd_read_settings(str(sf).encode(), C.byref(st)) == 0
+    cfg = G.Config()
+    assert L.cfd_settings_config(C.byref(st), C.byref(cfg)) == 0
+    grid = np.zeros(cfg.ghosted_shape())
+    gp = grid.ctypes.data_as(C.POINTER(C.c_double))
+    assert L.cfd_settings_ic(C.byref(st), C.byref(cfg), gp) == 0
+    p, model = params_from_config(cfg)
+    taken, n, t, _ = O.port_run(model, p, grid, 10**7)
+    assert t == cfg.T
+    base = st.basename
+    assert L.cfd_write_state(C.byref(cfg), gp, base, t) == 0
+    assert L.cfd_write_schlieren(C.byref(cfg), gp, base, t) == 0
+    names = [f"-state-{t:f}.dat", f"-schlieren-{t:f}.dat"]
+    if model == "allaire":
+        assert L.cfd_write_lineout(C.byref(cfg), gp, base, n) == 0
+        names += [f"-lineoutx-{n}.dat", f"-lineouty-{n}.dat"]
+    prefix = base.decode().rsplit("/", 1)[1]
+    for suffix in names:
+        name = prefix + suffix
+        assert name in fx, name
+        assert (tmp_path / name).read_bytes() == fx[name].tobytes(), name
