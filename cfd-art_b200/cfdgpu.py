@@ -140,6 +140,11 @@ def lib() -> C.CDLL:
             "cfd_get_status": (ip, [vp, C.POINTER(Status)]),
             "cfd_reset_counters": (ip, [vp]),
             "cfd_set_reference_ghosts": (ip, [vp, ip]),
+            "cfd_checkpoint_save": (ip, [vp, C.c_char_p]),
+            "cfd_checkpoint_load": (ip, [vp, C.c_char_p]),
+            "cfd_checkpoint_info": (ip, [C.c_char_p, cfgp, C.POINTER(ip), dp]),
+            "cfd_batch_save": (ip, [vp, ip, C.c_char_p]),
+            "cfd_batch_restore": (ip, [vp, C.c_char_p, ip, C.POINTER(ip)]),
             "cfd_set_kernel_timing": (ip, [vp, ip]),
             "cfd_kernel_times": (ip, [vp, dp, C.POINTER(ip)]),
             "cfd_reset_kernel_times": (ip, [vp]),
@@ -236,6 +241,16 @@ def recipe_ic(cfg: Config, name: str, seed: int = 20261203, nbubbles: int = 32) 
     return grid
 
 
+def checkpoint_info(path) -> tuple[Config, int, float]:
+    """Configuration, step count and time stored in a checkpoint file."""
+    cfg = Config()
+    n = C.c_int()
+    t = C.c_double()
+    check(lib().cfd_checkpoint_info(str(path).encode(), C.byref(cfg), C.byref(n), C.byref(t)),
+          "cfd_checkpoint_info")
+    return cfg, n.value, t.value
+
+
 def face_flux(cfg: Config, stencils: np.ndarray, dt: float, dx: float):
     """Device flux of independent faces: stencils (nfaces, 4|2, nvar)."""
     st = np.ascontiguousarray(stencils, dtype=np.float64)
@@ -291,6 +306,12 @@ class Solver:
         """Builds a named test case's initial condition on the device."""
         check(lib().cfd_upload_case(self._h, test_case.encode(), seed, n, t),
               f"cfd_upload_case({test_case})")
+
+    def save(self, path) -> None:
+        check(lib().cfd_checkpoint_save(self._h, str(path).encode()), "cfd_checkpoint_save")
+
+    def load(self, path) -> None:
+        check(lib().cfd_checkpoint_load(self._h, str(path).encode()), "cfd_checkpoint_load")
 
     def set_reference_ghosts(self, enable: bool = True) -> None:
         check(lib().cfd_set_reference_ghosts(self._h, int(enable)), "cfd_set_reference_ghosts")
@@ -409,6 +430,17 @@ class Batch:
         check(lib().cfd_batch_add_recipe(self._h, C.byref(cfg), RECIPE[name], seed, nbubbles,
                                          max_steps, C.byref(i)), "cfd_batch_add_recipe")
         self.cfgs[i.value] = cfg.copy()
+        return i.value
+
+    def save(self, mid: int, path) -> None:
+        check(lib().cfd_batch_save(self._h, mid, str(path).encode()), "cfd_batch_save")
+
+    def restore(self, path, max_steps: int = -1) -> int:
+        i = C.c_int()
+        check(lib().cfd_batch_restore(self._h, str(path).encode(), max_steps, C.byref(i)),
+              "cfd_batch_restore")
+        cfg, _, _ = checkpoint_info(path)
+        self.cfgs[i.value] = cfg
         return i.value
 
     def try_add(self, cfg: Config, grid: np.ndarray, max_steps: int = 0) -> int | None:

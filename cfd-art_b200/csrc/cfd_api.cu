@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/cfdgpu.h"
+#include "cfd_checkpoint.h"
 #include "cfd_error.h"
 #include "cfd_frame.h"
 #include "cfd_ic.h"
@@ -236,10 +237,8 @@ int enqueue_step(cfd_solver* s, bool host_dt, double dt) {
     // reference ghost values: the buffer current after the step keeps the
     // fill made before the sweep that read it last (naive: the x sweep;
     // Strang: the y sweep)
-    if (s->ref_ghosts &&
-        (r = enqueue_frame_snapshot(s, c.splitting == CFD_SPLIT_NAIVE ? 0 : 1, host_dt)))
-        return r;
     if (c.splitting == CFD_SPLIT_NAIVE) {
+        if (s->ref_ghosts && (r = enqueue_frame_snapshot(s, 0, host_dt))) return r;
         SweepArgs ax = sweep_args(s, DIR_X, 0, 1.0, host_dt, dt, false, false);
         if ((r = timed_sweep(s, DIR_X, ax, bx))) return r;
         SweepArgs ay = sweep_args(s, DIR_Y, 1, 1.0, host_dt, dt, true, false);
@@ -247,6 +246,7 @@ int enqueue_step(cfd_solver* s, bool host_dt, double dt) {
     }
     SweepArgs a1 = sweep_args(s, DIR_X, 0, 0.5, host_dt, dt, false, false);
     if ((r = timed_sweep(s, DIR_X, a1, bx))) return r;
+    if (s->ref_ghosts && (r = enqueue_frame_snapshot(s, 1, host_dt))) return r;
     SweepArgs a2 = sweep_args(s, DIR_Y, 1, 1.0, host_dt, dt, false, false);
     if ((r = timed_sweep(s, DIR_Y, a2, by))) return r;
     SweepArgs a3 = sweep_args(s, DIR_X, 0, 0.5, host_dt, dt, true, true);
@@ -860,6 +860,116 @@ int cfd_advance(cfd_solver* s, int max_steps) {
     }
     for (int i = 0; i < max_steps % K; ++i)
         if ((r = enqueue_step(s, false, 0.0))) return r;
+    return CFD_OK;
+}
+
+// ---- checkpoint / resume --------------------------------------------------
+
+int cfd_checkpoint_save(cfd_solver* s, const char* path) {
+    if (!s || !path) return fail(CFD_ERR_INVALID, "null argument");
+    if (!s->uploaded) return fail(CFD_ERR_STATE, "no state uploaded");
+    const cfd_config& c = s->cfg;
+    DevState d;
+    CkptHeader h;
+    ckpt_init(h);
+    CUDA_TRY(cudaMemcpyAsync(&d, s->dst, sizeof d, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(h.counters, s->counters, sizeof h.counters, cudaMemcpyDeviceToHost,
+                             s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    h.cfg = c;
+    h.cfg.stream = nullptr;
+    h.nv = s->nv;
+    h.g = s->g;
+    h.n = d.n;
+    h.done = d.done;
+    h.t = d.t;
+    h.dt = d.dt;
+    h.maxu = d.maxu;
+    h.maxv = d.maxv;
+    h.mass1 = d.mass1;
+    h.mass2 = d.mass2;
+    h.has_frame = s->frame != nullptr;
+    const size_t cells = (size_t)c.nx * c.ny;
+    const size_t fcells = s->frame ? (size_t)frame_cells(c.nx, c.ny, s->g) : 0;
+    h.state_bytes = sizeof(double) * s->nv * cells;
+    h.frame_bytes = sizeof(double) * s->nv * fcells;
+    std::vector<double> host(s->nv * cells + s->nv * fcells);
+    const double* src = s->buf[d.cur & 1];
+    for (int k = 0; k < s->nv; ++k)
+        CUDA_TRY(cudaMemcpy2DAsync(host.data() + k * cells, c.nx * sizeof(double),
+                                   src + k * s->plane, s->pitch * sizeof(double),
+                                   c.nx * sizeof(double), c.ny, cudaMemcpyDeviceToHost, s->stream));
+    if (s->frame)
+        CUDA_TRY(cudaMemcpyAsync(host.data() + s->nv * cells, s->frame, h.frame_bytes,
+                                 cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(CFD_ERR_INVALID, "cannot write %s", path);
+    bool ok = fwrite(&h, sizeof h, 1, f) == 1 &&
+              fwrite(host.data(), sizeof(double), host.size(), f) == host.size();
+    ok = (fclose(f) == 0) && ok;
+    return ok ? CFD_OK : fail(CFD_ERR_INVALID, "short write to %s", path);
+}
+
+int cfd_checkpoint_load(cfd_solver* s, const char* path) {
+    if (!s || !path) return fail(CFD_ERR_INVALID, "null argument");
+    const cfd_config& c = s->cfg;
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(CFD_ERR_INVALID, "cannot open %s", path);
+    CkptHeader h;
+    int r = ckpt_read_header(f, h);
+    if (r) {
+        fclose(f);
+        return fail(r, "%s is not a checkpoint", path);
+    }
+    if (h.cfg.precision != CFD_PREC_FP64 || h.cfg.model != c.model || h.cfg.nx != c.nx ||
+        h.cfg.ny != c.ny || h.g != s->g || h.cfg.dx != c.dx || h.cfg.dy != c.dy) {
+        fclose(f);
+        return fail(CFD_ERR_INVALID, "checkpoint %s holds a different solve", path);
+    }
+    const size_t cells = (size_t)c.nx * c.ny;
+    const size_t fcells = (size_t)frame_cells(c.nx, c.ny, s->g);
+    if (h.state_bytes != sizeof(double) * s->nv * cells ||
+        (h.has_frame && h.frame_bytes != sizeof(double) * s->nv * fcells)) {
+        fclose(f);
+        return fail(CFD_ERR_INVALID, "checkpoint %s has inconsistent sizes", path);
+    }
+    std::vector<double> host(s->nv * cells + (h.has_frame ? s->nv * fcells : 0));
+    bool ok = fread(host.data(), sizeof(double), host.size(), f) == host.size();
+    fclose(f);
+    if (!ok) return fail(CFD_ERR_INVALID, "checkpoint %s is truncated", path);
+    for (int k = 0; k < s->nv; ++k)
+        CUDA_TRY(cudaMemcpy2DAsync(s->buf[0] + k * s->plane, s->pitch * sizeof(double),
+                                   host.data() + k * cells, c.nx * sizeof(double),
+                                   c.nx * sizeof(double), c.ny, cudaMemcpyHostToDevice, s->stream));
+    DevState d;
+    memset(&d, 0, sizeof d);
+    d.t = h.t;
+    d.dt = h.dt;
+    d.T = c.T;
+    d.cfl = c.cfl;
+    d.maxu = h.maxu;
+    d.maxv = h.maxv;
+    d.mass1 = h.mass1;
+    d.mass2 = h.mass2;
+    d.dx = c.dx;
+    d.dy = c.dy;
+    d.n = h.n;
+    d.done = h.t >= c.T;
+    CUDA_TRY(cudaMemcpyAsync(s->dst, &d, sizeof d, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->counters, h.counters, sizeof h.counters, cudaMemcpyHostToDevice,
+                             s->stream));
+    if (s->frame) {
+        if (h.has_frame)
+            CUDA_TRY(cudaMemcpyAsync(s->frame, host.data() + s->nv * cells,
+                                     sizeof(double) * s->nv * fcells, cudaMemcpyHostToDevice,
+                                     s->stream));
+        else if ((r = frame_from_state(s)))
+            return r;
+    }
+    // the host vectors are pageable: the copies have read them when the calls return
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->uploaded = true;
     return CFD_OK;
 }
 

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/cfdgpu.h"
+#include "cfd_checkpoint.h"
 #include "cfd_error.h"
 #include "cfd_ic.h"
 #include "cfd_mixed.cuh"
@@ -460,9 +461,17 @@ int cfd_batch_member_bytes(const cfd_config* cfg, size_t* bytes) {
 
 // Adds a member whose initial state is either a ghosted AoS host grid or a
 // shape program built on the device.
+// Saved state of a member (cfd_batch_restore): packed value and
+// compensation planes (nx * ny cells each, no padding) and its time state.
+struct Restore {
+    const CkptHeader* h;
+    const float4* q4[2];
+    const float2* q2[2];
+};
+
 static int add_member(cfd_batch* b, const cfd_config* cfg, const double* host_ic,
                       const std::vector<cfdic::Op>* prog, const cfdic::Eos* prog_eos,
-                      int max_steps, int* id_out) {
+                      int max_steps, int* id_out, const Restore* rs = nullptr) {
     const cfd_config& c = *cfg;
     if (c.model != CFD_MODEL_EULER && c.model != CFD_MODEL_ALLAIRE)
         return cfd_fail(CFD_ERR_INVALID, "unknown model %d", c.model);
@@ -546,9 +555,9 @@ static int add_member(cfd_batch* b, const cfd_config* cfg, const double* host_ic
     // initial wave-speed reduction reads
     int g = c.flux_solver == CFD_FLUX_GODUNOV ? 1 : 2;
     size_t ghosted = host_ic ? (size_t)nv * (c.nx + 2 * g) * (size_t)(c.ny + 2 * g) : 0;
-    size_t soa = (size_t)nv * plane;
+    size_t soa = rs ? 0 : (size_t)nv * plane;
     double* staging = nullptr;
-    cudaError_t e = cudaMalloc(&staging, sizeof(double) * (ghosted + soa));
+    cudaError_t e = rs ? cudaSuccess : cudaMalloc(&staging, sizeof(double) * (ghosted + soa));
     if (e != cudaSuccess) {
         cudaFree(m.mem);
         return cfd_fail(CFD_ERR_NOMEM, "staging: %s", cudaGetErrorString(e));
@@ -559,8 +568,33 @@ static int add_member(cfd_batch* b, const cfd_config* cfg, const double* host_ic
     init.cfl = c.cfl;
     init.dx = c.dx;
     init.dy = c.dy;
+    if (rs) {  // the saved time state, current state in buffer 0
+        init.t = rs->h->t;
+        init.dt = rs->h->dt;
+        init.maxu = rs->h->maxu;
+        init.maxv = rs->h->maxv;
+        init.mass1 = rs->h->mass1;
+        init.mass2 = rs->h->mass2;
+        init.n = rs->h->n;
+        init.done = rs->h->t >= c.T;
+    }
     int r = CFD_OK;
     do {
+        if (rs) {
+            for (int w = 0; w < 2 && !e; ++w) {
+                e = cudaMemcpy2DAsync(I.q4[0][w], pitch * sizeof(float4), rs->q4[w],
+                                      c.nx * sizeof(float4), c.nx * sizeof(float4), c.ny,
+                                      cudaMemcpyHostToDevice, b->stream);
+                if (!e && nv == 6)
+                    e = cudaMemcpy2DAsync(I.q2[0][w], pitch * sizeof(float2), rs->q2[w],
+                                          c.nx * sizeof(float2), c.nx * sizeof(float2), c.ny,
+                                          cudaMemcpyHostToDevice, b->stream);
+            }
+            if (!e) e = cudaMemcpyAsync(I.st, &init, sizeof init, cudaMemcpyHostToDevice, b->stream);
+            if (!e) e = cudaStreamSynchronize(b->stream);
+            if (e) r = cfd_fail(CFD_ERR_CUDA, "restore: %s", cudaGetErrorString(e));
+            break;
+        }
         if ((e = cudaMemcpyAsync(I.st, &init, sizeof init, cudaMemcpyHostToDevice, b->stream))) {
             r = cfd_fail(CFD_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
             break;
@@ -804,6 +838,113 @@ int cfd_batch_poll(cfd_batch* b, int cap, int* ids, int* steps, int* done, doubl
         if (t) t[i] = ds[i].t;
     }
     return CFD_OK;
+}
+
+int cfd_batch_save(cfd_batch* b, int id, const char* path) {
+    if (!b || !path) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    Member* m = find(b, id);
+    if (!m) return cfd_fail(CFD_ERR_INVALID, "no instance %d", id);
+    const cfd_config& c = m->cfg;
+    const Inst& I = m->inst;
+    DevState d;
+    BTRY(cudaMemcpyAsync(&d, I.st, sizeof d, cudaMemcpyDeviceToHost, b->stream));
+    BTRY(cudaStreamSynchronize(b->stream));
+    const int cur = d.cur & 1, nv = I.nv;
+    const size_t cells = (size_t)c.nx * c.ny;
+    std::vector<float4> q4[2];
+    std::vector<float2> q2[2];
+    for (int w = 0; w < 2; ++w) {
+        q4[w].resize(cells);
+        BTRY(cudaMemcpy2DAsync(q4[w].data(), c.nx * sizeof(float4), I.q4[cur][w],
+                               I.pitch * sizeof(float4), c.nx * sizeof(float4), c.ny,
+                               cudaMemcpyDeviceToHost, b->stream));
+        if (nv == 6) {
+            q2[w].resize(cells);
+            BTRY(cudaMemcpy2DAsync(q2[w].data(), c.nx * sizeof(float2), I.q2[cur][w],
+                                   I.pitch * sizeof(float2), c.nx * sizeof(float2), c.ny,
+                                   cudaMemcpyDeviceToHost, b->stream));
+        }
+    }
+    BTRY(cudaStreamSynchronize(b->stream));
+    // packed cells -> planes: values of components 0..nv-1, then their compensations
+    std::vector<float> planes(2 * nv * cells);
+    for (int w = 0; w < 2; ++w)
+        for (size_t q = 0; q < cells; ++q) {
+            float* p = planes.data() + (size_t)w * nv * cells + q;
+            p[0] = q4[w][q].x;
+            p[cells] = q4[w][q].y;
+            p[2 * cells] = q4[w][q].z;
+            p[3 * cells] = q4[w][q].w;
+            if (nv == 6) {
+                p[4 * cells] = q2[w][q].x;
+                p[5 * cells] = q2[w][q].y;
+            }
+        }
+    CkptHeader h;
+    ckpt_init(h);
+    h.cfg = c;
+    h.cfg.stream = nullptr;
+    h.cfg.precision = CFD_PREC_MIXED;
+    h.nv = nv;
+    h.g = c.flux_solver == CFD_FLUX_GODUNOV ? 1 : 2;
+    h.n = d.n;
+    h.done = d.done;
+    h.t = d.t;
+    h.dt = d.dt;
+    h.maxu = d.maxu;
+    h.maxv = d.maxv;
+    h.mass1 = d.mass1;
+    h.mass2 = d.mass2;
+    h.max_steps = m->max_steps;
+    h.state_bytes = sizeof(float) * planes.size();
+    FILE* f = fopen(path, "wb");
+    if (!f) return cfd_fail(CFD_ERR_INVALID, "cannot write %s", path);
+    bool ok = fwrite(&h, sizeof h, 1, f) == 1 &&
+              fwrite(planes.data(), sizeof(float), planes.size(), f) == planes.size();
+    ok = (fclose(f) == 0) && ok;
+    return ok ? CFD_OK : cfd_fail(CFD_ERR_INVALID, "short write to %s", path);
+}
+
+int cfd_batch_restore(cfd_batch* b, const char* path, int max_steps, int* id_out) {
+    if (!b || !path || !id_out) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    FILE* f = fopen(path, "rb");
+    if (!f) return cfd_fail(CFD_ERR_INVALID, "cannot open %s", path);
+    CkptHeader h;
+    int r = ckpt_read_header(f, h);
+    const int nv = h.nv;
+    const size_t cells = r ? 0 : (size_t)h.cfg.nx * h.cfg.ny;
+    if (!r && (h.cfg.precision != CFD_PREC_MIXED || h.cfg.model != (nv == 4 ? 0 : 1) ||
+               h.state_bytes != sizeof(float) * 2 * nv * cells))
+        r = CFD_ERR_INVALID;
+    std::vector<float> planes;
+    if (!r) {
+        planes.resize(2 * nv * cells);
+        if (fread(planes.data(), sizeof(float), planes.size(), f) != planes.size())
+            r = CFD_ERR_INVALID;
+    }
+    fclose(f);
+    if (r) return cfd_fail(r, "%s is not a mixed-precision checkpoint", path);
+    std::vector<float4> q4[2];
+    std::vector<float2> q2[2];
+    for (int w = 0; w < 2; ++w) {
+        q4[w].resize(cells);
+        if (nv == 6) q2[w].resize(cells);
+        for (size_t q = 0; q < cells; ++q) {
+            const float* p = planes.data() + (size_t)w * nv * cells + q;
+            q4[w][q] = make_float4(p[0], p[cells], p[2 * cells], p[3 * cells]);
+            if (nv == 6) q2[w][q] = make_float2(p[4 * cells], p[5 * cells]);
+        }
+    }
+    Restore rs;
+    rs.h = &h;
+    for (int w = 0; w < 2; ++w) {
+        rs.q4[w] = q4[w].data();
+        rs.q2[w] = nv == 6 ? q2[w].data() : nullptr;
+    }
+    cfd_config c = h.cfg;
+    c.stream = nullptr;
+    return add_member(b, &c, nullptr, nullptr, nullptr, max_steps < 0 ? h.max_steps : max_steps,
+                      id_out, &rs);
 }
 
 int cfd_batch_download(cfd_batch* b, int id, double* host, int layout) {

@@ -9,6 +9,7 @@
 
 #include "../../include/cfdgpu.h"
 #include "../../include/cfdgpu_host.h"
+#include "cfd_checkpoint.h"
 
 namespace {
 
@@ -239,6 +240,20 @@ int cfd_write_lineout(const cfd_config* c, const double* grid, const char* basen
     if (!oy) return CFD_ERR_INVALID;
     int j = v.nx / 2;
     for (int r = 0; r < v.ny + 2 * v.g; ++r) line(oy, v.ccy(r), v.cell(r, j));
+    return CFD_OK;
+}
+
+int cfd_checkpoint_info(const char* path, cfd_config* cfg, int* n, double* t) {
+    if (!path) return CFD_ERR_INVALID;
+    FILE* f = fopen(path, "rb");
+    if (!f) return CFD_ERR_INVALID;
+    cfd::CkptHeader h;
+    int r = cfd::ckpt_read_header(f, h);
+    fclose(f);
+    if (r) return r;
+    if (cfg) *cfg = h.cfg;
+    if (n) *n = h.n;
+    if (t) *t = h.t;
     return CFD_OK;
 }
 

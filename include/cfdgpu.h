@@ -134,6 +134,19 @@ int cfd_upload_case(cfd_solver* s, const char* test_case, uint64_t seed, int n, 
  * the ghost strips hold the boundary fill of the current state. */
 int cfd_download(cfd_solver* s, double* host, int layout);
 
+/* Checkpoint / resume.  cfd_checkpoint_save writes the current state, the
+ * device time-loop state (n, t, the dt chosen for the next step, wave speeds,
+ * masses), the event counters and the reference ghost values when kept, to a
+ * binary file (little-endian header + FP64 SoA planes); cfd_checkpoint_load
+ * reads it into a solver of the same model, grid and spacing, after which
+ * the solve continues bit for bit as if it had not stopped.  Synchronous.
+ * No counterpart in the reference, which runs each problem start to end. */
+int cfd_checkpoint_save(cfd_solver* s, const char* path);
+int cfd_checkpoint_load(cfd_solver* s, const char* path);
+/* Reads a checkpoint's header (plain FP64 or batch member): its
+ * configuration, step count and time.  Host only. */
+int cfd_checkpoint_info(const char* path, cfd_config* cfg, int* n, double* t);
+
 /* Keeps the ghost values the reference's grid holds between boundary fills,
  * for output writers that read ghost cells (the schlieren stencil at the
  * domain edge, the Allaire lineouts): after an upload, the uploaded grid's
@@ -232,6 +245,12 @@ int cfd_batch_add(cfd_batch* b, const cfd_config* cfg, const double* host_ic, in
 int cfd_batch_add_recipe(cfd_batch* b, const cfd_config* cfg, int recipe, uint64_t seed,
                          int nbubbles, int max_steps, int* id_out);
 int cfd_batch_remove(cfd_batch* b, int id);
+/* Saves a member (configuration, FP32 value and compensation planes, time
+ * state, step limit) to a checkpoint file; cfd_batch_restore adds it back,
+ * to this or another batch, continuing bit for bit (max_steps < 0: the
+ * saved step limit).  Lets a server evict a solve and resume it later. */
+int cfd_batch_save(cfd_batch* b, int id, const char* path);
+int cfd_batch_restore(cfd_batch* b, const char* path, int max_steps, int* id_out);
 int cfd_batch_size(cfd_batch* b, int* count, size_t* used_bytes, size_t* budget_bytes);
 /* Advances every member by `ticks` steps (members that are done idle). */
 int cfd_batch_step(cfd_batch* b, int ticks);

@@ -179,3 +179,12 @@ def test_output_writers_match_reference(tmp_path, model, case):
             a, b = tmp_path / f"ref-{kind}-5.dat", tmp_path / f"ours-{kind}-5.dat"
             assert a.exists() and b.exists()
             assert filecmp.cmp(a, b, shallow=False), kind
+
+
+def test_checkpoint_info_rejects_non_checkpoints(tmp_path):
+    f = tmp_path / "x.ckpt"
+    f.write_bytes(b"CFDCKPT\0" + b"\0" * 16)
+    with pytest.raises(G.CfdError):
+        G.checkpoint_info(f)
+    with pytest.raises(G.CfdError):
+        G.checkpoint_info(tmp_path / "missing.ckpt")
