@@ -263,7 +263,7 @@ struct cfd_batch {
     Inst* d_insts = nullptr;
     int d_insts_cap = 0;
     // tile lists per (model, dir): device arrays
-    int* d_tiles = nullptr;
+    TileEnt* d_tiles = nullptr;
     size_t d_tiles_cap = 0;
     struct Group {
         int model, dir, shape, ntiles, offset;
@@ -284,7 +284,6 @@ namespace {
 
 int build_tables(cfd_batch* b) {
     if (!b->dirty) return CFD_OK;
-    std::vector<int> all;
     b->groups.clear();
     std::vector<Inst> insts(b->members.size());
     for (size_t i = 0; i < b->members.size(); ++i) {
@@ -302,30 +301,37 @@ int build_tables(cfd_batch* b) {
         return (long long)b->members[x].cfg.nx * b->members[x].cfg.ny >
                (long long)b->members[y].cfg.nx * b->members[y].cfg.ny;
     });
+    std::vector<TileEnt> all;
     for (int model = 0; model < 2; ++model)
         for (int dir = 0; dir < 2; ++dir) {
             cfd_batch::Group g;
             g.model = model;
             g.dir = dir;
             g.shape = b->shape[model][dir];
-            g.offset = (int)all.size() / 2;
-            std::vector<int> ti, tl;
+            g.offset = (int)all.size();
+            const Shape sh = dir == DIR_X ? kShapesX[g.shape] : kShapesY[g.shape];
             for (int idx : order) {
                 const Member& m = b->members[idx];
                 if (m.cfg.model != model) continue;
-                int nt = dir == DIR_X ? insts[idx].tiles_x : insts[idx].tiles_y;
+                const int len = dir == DIR_X ? m.cfg.nx : m.cfg.ny;
+                const int wid = dir == DIR_X ? m.cfg.ny : m.cfg.nx;
+                const int along = (len + sh.ts - 1) / sh.ts;
+                const int nt = dir == DIR_X ? insts[idx].tiles_x : insts[idx].tiles_y;
                 for (int t = 0; t < nt; ++t) {
-                    ti.push_back(idx);
-                    tl.push_back(t);
+                    TileEnt e;
+                    e.inst = idx;
+                    e.local = t;
+                    e.a_org = (t % along) * sh.ts - 2;
+                    e.b_org = (t / along) * sh.na;
+                    e.len = len;
+                    e.wid = wid;
+                    e.max_steps = insts[idx].max_steps;
+                    e.active = insts[idx].active;
+                    all.push_back(e);
                 }
             }
-            g.ntiles = (int)ti.size();
-            if (!g.ntiles) continue;
-            // store as [inst..., local...] pairs: inst at offset, local at offset + ntiles
-            g.offset = (int)all.size();
-            all.insert(all.end(), ti.begin(), ti.end());
-            all.insert(all.end(), tl.begin(), tl.end());
-            b->groups.push_back(g);
+            g.ntiles = (int)all.size() - g.offset;
+            if (g.ntiles) b->groups.push_back(g);
         }
     if ((int)insts.size() > b->d_insts_cap) {
         cudaFree(b->d_insts);
@@ -338,14 +344,14 @@ int build_tables(cfd_batch* b) {
         cudaFree(b->d_tiles);
         b->d_tiles = nullptr;
         size_t cap = std::max<size_t>(1024, all.size() * 2);
-        BTRY(cudaMalloc(&b->d_tiles, sizeof(int) * cap));
+        BTRY(cudaMalloc(&b->d_tiles, sizeof(TileEnt) * cap));
         b->d_tiles_cap = cap;
     }
     if (!insts.empty())
         BTRY(cudaMemcpyAsync(b->d_insts, insts.data(), sizeof(Inst) * insts.size(),
                              cudaMemcpyHostToDevice, b->stream));
     if (!all.empty())
-        BTRY(cudaMemcpyAsync(b->d_tiles, all.data(), sizeof(int) * all.size(),
+        BTRY(cudaMemcpyAsync(b->d_tiles, all.data(), sizeof(TileEnt) * all.size(),
                              cudaMemcpyHostToDevice, b->stream));
     BTRY(cudaStreamSynchronize(b->stream));  // host vectors die at return
     if (b->graph) {
@@ -368,8 +374,7 @@ int enqueue_tick(cfd_batch* b, std::vector<Timed>* timing) {
             if (g.dir != dir) continue;
             MixedArgs a;
             a.insts = b->d_insts;
-            a.tile_inst = b->d_tiles + g.offset;
-            a.tile_local = b->d_tiles + g.offset + g.ntiles;
+            a.tiles = b->d_tiles + g.offset;
             a.ntiles = g.ntiles;
             cudaEvent_t e0 = nullptr, e1 = nullptr;
             if (timing) {
@@ -548,6 +553,8 @@ static int add_member(cfd_batch* b, const cfd_config* cfg, const double* host_ic
     const bool stiff = I.eos.p1 != 0.0 || (c.model == CFD_MODEL_ALLAIRE && I.eos.p2 != 0.0);
     I.flags = (c.limiter & 3) | (c.wavespeed == CFD_WS_PVRS ? MF_PVRS : 0) |
               (I.godunov ? MF_GODUNOV : 0) | (stiff ? MF_STIFF : 0);
+    for (int k = 0; k < 4; ++k)
+        if (c.bc[k] == CFD_BC_REFLECTIVE) I.flags |= MF_BC << k;
     I.max_steps = max_steps;
     I.active = 1;
     // upload: the ghosted FP64 grid (or the device-built SoA state) goes

@@ -43,7 +43,8 @@ struct Inst {
     // FP32 constants of the sweeps (loaded into registers once per tile):
     // g1, p1, g1 - 1, g1 p1, 1/(g1 - 1), 1/(g2 - 1), g1 p1/(g1 - 1), g2 p2/(g2 - 1)
     alignas(16) float pf[8];
-    int flags;       // limiter (bits 0-1), PVRS speeds (2), Godunov (3), stiffened gas (4)
+    int flags;       // limiter (bits 0-1), PVRS speeds (2), Godunov (3), stiffened gas (4),
+                     // reflective walls L, R, B, T (5-8)
     // FP64 mixture constants for the pressure of stiffened-gas cells:
     // 1/(g1 - 1), 1/(g2 - 1), g1 p1/(g1 - 1), g2 p2/(g2 - 1)
     double pd[4];
@@ -54,10 +55,19 @@ struct Inst {
     int active;             // 0: skip
 };
 
+// One tile of a launch, precomputed on the host when the membership or the
+// tile shapes change.
+struct alignas(16) TileEnt {
+    int inst;          // instance
+    int local;         // tile index within the instance
+    int a_org, b_org;  // first staged cell along the sweep (halo included), first line
+    int len, wid;      // cells along the sweep and lines of the instance
+    int max_steps, active;
+};
+
 struct MixedArgs {
     Inst* insts;
-    const int* tile_inst;   // instance of each tile of this launch
-    const int* tile_local;  // tile index within its instance
+    const TileEnt* tiles;   // tiles of this launch
     int ntiles;             // tiles of this launch
     int chunk;              // CTA c walks tiles [c * chunk, (c + 1) * chunk) (persistent)
 };
@@ -72,7 +82,7 @@ struct MPar {
     __device__ __forceinline__ bool godunov() const { return (flags >> 3) & 1; }
     __device__ __forceinline__ bool stiff() const { return (flags >> 4) & 1; }
 };
-enum { MF_PVRS = 4, MF_GODUNOV = 8, MF_STIFF = 16 };
+enum { MF_PVRS = 4, MF_GODUNOV = 8, MF_STIFF = 16, MF_BC = 32 };  // MF_BC << k: wall on side k (L, R, B, T)
 
 __device__ __forceinline__ MPar load_par(const Inst& I) {
     const float4 a = *reinterpret_cast<const float4*>(I.pf);
@@ -83,6 +93,18 @@ __device__ __forceinline__ MPar load_par(const Inst& I) {
     P.flags = I.flags;
     return P;
 }
+
+// Asynchronous global -> shared copies (no registers held while in flight).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 __device__ __forceinline__ float frcp(float x) { return 1.0f / x; }
 __device__ __forceinline__ float fdiv(float a, float b) { return a / b; }
@@ -266,7 +288,7 @@ __device__ __forceinline__ void hllc_prim(const MPar& P, const float* WL, const 
     float dSL = SL - uL, dSR = SR - uR;
     float us = fdiv((pR - pL) + rL * uL * dSL - rR * uR * dSR, rL * dSL - rR * dSR);
     bool left = !signbit(us);
-    const float* W = left ? WL : WR;
+    // per-element selects (a pointer to either side would put both in local memory)
     float rho = left ? rL : rR, u = left ? uL : uR, p = left ? pL : pR;
     float Sk = left ? SL : SR, dS = left ? dSL : dSR;
     float wave = left ? fminf_s(0.0f, SL) : fmaxf_s(0.0f, SR);
@@ -274,20 +296,20 @@ __device__ __forceinline__ void hllc_prim(const MPar& P, const float* WL, const 
     // conserved state of the selected side
     float U[NV];
     if constexpr (MODEL == MODEL_EULER) {
-        float v = W[2];
+        float v = left ? WL[2] : WR[2];
         U[0] = rho;
         U[1] = rho * u;
         U[2] = rho * v;
         U[3] = (p + P.gp1) * P.i1 + 0.5f * rho * (u * u + v * v);
     } else {
-        float v = W[3];
+        float v = left ? WL[3] : WR[3];
         float eps = left ? epsL : epsR, k = left ? kL : kR;
-        U[0] = W[0];
-        U[1] = W[1];
+        U[0] = left ? WL[0] : WR[0];
+        U[1] = left ? WL[1] : WR[1];
         U[2] = rho * u;
         U[3] = rho * v;
         U[4] = (p + k) * eps + 0.5f * rho * (u * u + v * v);
-        U[5] = W[5];
+        U[5] = left ? WL[5] : WR[5];
     }
     float Us[NV];
 #pragma unroll
@@ -388,8 +410,11 @@ struct MTile {
             b = i - (i / NA) * NA;
         }
     }
-    // vectors per slot: value, compensation, W, W+, W-, flux; u*, z*; flags
-    static constexpr int SMEM = 6 * VB * NSLOT + 8 * NSLOT + NSLOT + 64;
+    // vectors per slot: value, compensation, W, W+, W-, flux; u*, z*; flags;
+    // then the staging area the next tile's cells are copied into
+    // (value and compensation, slot = thread)
+    static constexpr int STG = (6 * VB * NSLOT + 8 * NSLOT + NSLOT + 15) / 16 * 16;
+    static constexpr int SMEM = STG + 2 * VB * NSLOT;
 };
 
 // Where a tile lies and whether it is skipped.
@@ -400,41 +425,47 @@ struct TileGeom {
 
 template <int DIR, int TS, int NA>
 __device__ __forceinline__ TileGeom tile_geom(const MixedArgs& A, int tile) {
+    const int4* e = reinterpret_cast<const int4*>(A.tiles + tile);
+    const int4 e0 = e[0], e1 = e[1];
     TileGeom g;
-    g.inst = A.tile_inst[tile];
-    g.ltile = A.tile_local[tile];
-    const Inst& I = A.insts[g.inst];
-    const DevState* st = I.st;
-    g.skip = !I.active || st->done || st->n >= I.max_steps;
+    g.inst = e0.x;
+    g.ltile = e0.y;
+    g.a_org = e0.z;
+    g.b_org = e0.w;
+    g.len = e1.x;
+    g.wid = e1.y;
+    const DevState* st = A.insts[g.inst].st;
+    g.skip = !e1.w || st->done || st->n >= e1.z;
     g.cur = st->cur;
-    g.len = (DIR == DIR_X) ? I.nx : I.ny;
-    g.wid = (DIR == DIR_X) ? I.ny : I.nx;
-    int tiles_along = (g.len + TS - 1) / TS;
-    g.a_org = (g.ltile % tiles_along) * TS - 2;
-    g.b_org = (g.ltile / tiles_along) * NA;
     return g;
 }
 
-// This thread's staged cell of a tile (with the boundary mirror): loads it
-// into registers; `neg` says whether the normal momentum must be negated.
+// Starts copying this thread's staged cell of a tile (the boundary mirror
+// of pre_sweep picks the source cell) into its staging slot.
 template <int MODEL, int DIR, int TS, int NA>
-__device__ __forceinline__ void tile_fetch(const MixedArgs& A, const TileGeom& g, float* h,
-                                           float* l, bool& neg) {
+__device__ __forceinline__ void tile_issue(const MixedArgs& A, const TileGeom& g, char* smem) {
     using Tl = MTile<MODEL, DIR, TS, NA>;
     const Inst& I = A.insts[g.inst];
     int a, b;
     Tl::item(threadIdx.x, 0, Tl::LA, a, b);
-    int ga = g.a_org + a, gb = g.b_org + b;
+    const int ga = g.a_org + a, gb = g.b_org + b;
     int src = ga;
-    neg = false;
-    int bc_lo = (DIR == DIR_X) ? I.bc[0] : I.bc[2];
-    int bc_hi = (DIR == DIR_X) ? I.bc[1] : I.bc[3];
-    if (ga < 0) { src = -ga - 1; neg = bc_lo; }
-    else if (ga >= g.len) { src = 2 * g.len - 1 - ga; neg = bc_hi; }
+    if (ga < 0) src = -ga - 1;
+    else if (ga >= g.len) src = 2 * g.len - 1 - ga;
     src = min(max(src, 0), g.len - 1);
-    int gbs = min(gb, g.wid - 1);
-    long long off = (DIR == DIR_X) ? (long long)gbs * I.pitch + src : (long long)src * I.pitch + gbs;
-    load_cell<MODEL>(I, g.cur ^ (DIR == DIR_Y), off, h, l);
+    const int gbs = min(gb, g.wid - 1);
+    const long long off =
+        (DIR == DIR_X) ? (long long)gbs * I.pitch + src : (long long)src * I.pitch + gbs;
+    const int buf = g.cur ^ (DIR == DIR_Y);
+    char* stg = smem + Tl::STG;
+    const int t = threadIdx.x;
+    cp_async16(stg + 16 * t, I.q4[buf][0] + off);
+    cp_async16(stg + 16 * (Tl::NSLOT + t), I.q4[buf][1] + off);
+    if constexpr (MODEL == MODEL_ALLAIRE) {
+        cp_async8(stg + 32 * Tl::NSLOT + 8 * t, I.q2[buf][0] + off);
+        cp_async8(stg + 40 * Tl::NSLOT + 8 * t, I.q2[buf][1] + off);
+    }
+    cp_async_commit();
 }
 
 // Per-thread wave-speed maxima and mass sums of the tiles of a run.
@@ -444,9 +475,9 @@ struct RAcc {
 };
 
 template <int MODEL, int DIR, int TS, int NA>
-__device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g, float* h,
-                                           float* l, bool& neg, int next_tile, char* smem,
-                                           RAcc& racc) {
+__device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g, int next_tile,
+                                           char* smem, RAcc& racc, TileGeom& s_next,
+                                           float* s_coef) {
     using Tl = MTile<MODEL, DIR, TS, NA>;
     using MT = ModelTraits<MODEL>;
     constexpr int NV = MT::NV, LA = Tl::LA, NSLOT = Tl::NSLOT, ST = Tl::ST;
@@ -463,17 +494,47 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
 
     const Inst& I = A.insts[g.inst];
     const MPar P = load_par(I);
-    DevState* st = I.st;
-    const double dt = st->dt;
-    const double h_flux = (DIR == DIR_X) ? I.dx : (I.fix_dy ? I.dy : I.dx);
-    const double h_upd = (DIR == DIR_X) ? I.dx : I.dy;
-    const float s_half = (float)(0.5 * (dt / h_flux));
-    const float k_upd = (float)(dt / h_upd);
+    // CTA-wide values of this tile, made once by thread 0 during P1 (shared
+    // memory): the sweep's coefficients and the geometry of the next tile
+    if (tid == 0) {
+        const double dt = I.st->dt;
+        const double h_flux = (DIR == DIR_X) ? I.dx : (I.fix_dy ? I.dy : I.dx);
+        const double h_upd = (DIR == DIR_X) ? I.dx : I.dy;
+        s_coef[0] = (float)(0.5 * (dt / h_flux));
+        s_coef[1] = (float)(dt / h_upd);
+        TileGeom t;
+        if (next_tile < A.ntiles) {
+            t = tile_geom<DIR, TS, NA>(A, next_tile);
+        } else {
+            t.inst = -1;
+            t.skip = true;
+        }
+        s_next = t;
+    }
 
     // ---- P1: boundary sign, rotation, conversion of the fetched cell -------
     {
         int a, b;
         Tl::item(tid, 0, LA, a, b);
+        float h[NV], l[NV];
+        cp_async_wait_all();
+        {
+            const char* stg = smem + Tl::STG;
+            const float4 x = *reinterpret_cast<const float4*>(stg + 16 * tid);
+            const float4 y = *reinterpret_cast<const float4*>(stg + 16 * (NSLOT + tid));
+            h[0] = x.x; h[1] = x.y; h[2] = x.z; h[3] = x.w;
+            l[0] = y.x; l[1] = y.y; l[2] = y.z; l[3] = y.w;
+            if constexpr (MODEL == MODEL_ALLAIRE) {
+                const float2 z = *reinterpret_cast<const float2*>(stg + 32 * NSLOT + 8 * tid);
+                const float2 w = *reinterpret_cast<const float2*>(stg + 40 * NSLOT + 8 * tid);
+                h[4] = z.x; h[5] = z.y;
+                l[4] = w.x; l[5] = w.y;
+            }
+        }
+        const int ga = g.a_org + a;
+        const int wall_lo = (DIR == DIR_X) ? 0 : 2;
+        const bool neg = (ga < 0 && ((P.flags >> (5 + wall_lo)) & 1)) ||
+                         (ga >= g.len && ((P.flags >> (6 + wall_lo)) & 1));
         if (DIR == DIR_X) {
             if (neg) { h[MT::IM] = -h[MT::IM]; l[MT::IM] = -l[MT::IM]; }
         } else {
@@ -489,12 +550,14 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
         sL.put(s, l);
         sW.put(s, W);
     }
-    // the registers are free: start loading this thread's cell of the next tile
-    if (next_tile < A.ntiles) {
-        TileGeom gn = tile_geom<DIR, TS, NA>(A, next_tile);
-        if (!gn.skip) tile_fetch<MODEL, DIR, TS, NA>(A, gn, h, l, neg);
-    }
     __syncthreads();
+    // the staging slot is free: start copying this thread's cell of the next tile
+    {
+        const TileGeom gn = s_next;
+        if (!gn.skip) tile_issue<MODEL, DIR, TS, NA>(A, gn, smem);
+    }
+    const float s_half = s_coef[0];
+    const float k_upd = s_coef[1];
 
     // ---- P2: slopes and evolved face states (primitive) ----------------
     if (!P.godunov() && tid < (LA - 2) * NA) {
@@ -564,21 +627,18 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
         int ga = g.a_org + a, gb = g.b_org + b;
         if (ga < g.len && gb < g.wid) {
             int s = Tl::slot(a, b);
-            float hh[NV], ll[NV], FL[NV], FR[NV];
+            float hh[NV], ll[NV];
             sH.get(s, hh);
             sL.get(s, ll);
-            sF.get(s, FL);
-            sF.get(s + ST, FR);
-            float oh[NV], ol[NV];
+            {
+                float FL[NV], FR[NV];
+                sF.get(s, FL);
+                sF.get(s + ST, FR);
 #pragma unroll
-            for (int k = 0; k < NV; ++k) {
-                oh[k] = hh[k];
-                ol[k] = ll[k];
-            }
-#pragma unroll
-            for (int k = 0; k < NV; ++k) {
-                if (MODEL == MODEL_ALLAIRE && k == 5) continue;
-                comp_add(hh[k], ll[k], k_upd * (FL[k] - FR[k]));
+                for (int k = 0; k < NV; ++k) {
+                    if (MODEL == MODEL_ALLAIRE && k == 5) continue;
+                    comp_add(hh[k], ll[k], k_upd * (FL[k] - FR[k]));
+                }
             }
             if constexpr (MODEL == MODEL_ALLAIRE) {
                 float2 uzL = sUZ[s], uzR = sUZ[s + ST];
@@ -602,16 +662,20 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
                 float t = hh[MT::IM], tl = ll[MT::IM];
                 hh[MT::IM] = -hh[MT::IT]; ll[MT::IM] = -ll[MT::IT];
                 hh[MT::IT] = t; ll[MT::IT] = tl;
-                float t2 = oh[MT::IM], t2l = ol[MT::IM];
-                oh[MT::IM] = -oh[MT::IT]; ol[MT::IM] = -ol[MT::IT];
-                oh[MT::IT] = t2; ol[MT::IT] = t2l;
             }
             float Wn[NV];
             c2p_mixed<MODEL>(I, P, hh, ll, Wn);
             if constexpr (MODEL == MODEL_EULER) {
                 // density / energy restore as in the plain form (rare)
                 if (!(hh[0] > 1e-12f) || !(Wn[3] + P.gp1 > 0.0f)) {
-                    float Wo[NV];
+                    float oh[NV], ol[NV], Wo[NV];  // the cell before the update
+                    sH.get(s, oh);
+                    sL.get(s, ol);
+                    if (DIR == DIR_Y) {
+                        float t2 = oh[MT::IM], t2l = ol[MT::IM];
+                        oh[MT::IM] = -oh[MT::IT]; ol[MT::IM] = -ol[MT::IT];
+                        oh[MT::IT] = t2; ol[MT::IT] = t2l;
+                    }
                     c2p_mixed<MODEL>(I, P, oh, ol, Wo);
                     float rho = hh[0] > 1e-12f ? hh[0] : oh[0];
                     float u = Wn[1], v = Wn[2];
@@ -703,42 +767,45 @@ __device__ __forceinline__ void flush_run(const MixedArgs& A, int inst, int slot
 template <int MODEL, int DIR, int TS, int NA>
 __global__ void __launch_bounds__(256, MODEL == MODEL_EULER ? 4 : 3) mixed_sweep_kernel(MixedArgs A) {
     extern __shared__ __align__(16) char msm[];
-    constexpr int NV = ModelTraits<MODEL>::NV;
-    float h[NV], l[NV];
-    bool neg = false;
+    __shared__ TileGeom s_next;
+    __shared__ float s_coef[2];
     const int t_begin = blockIdx.x * A.chunk;
     const int t_end = min(t_begin + A.chunk, A.ntiles);
     if (t_begin >= t_end) return;
     TileGeom g = tile_geom<DIR, TS, NA>(A, t_begin);
-    if (!g.skip) tile_fetch<MODEL, DIR, TS, NA>(A, g, h, l, neg);
+    if (!g.skip) tile_issue<MODEL, DIR, TS, NA>(A, g, msm);
     RAcc racc{0.0f, 0.0f, 0.0, 0.0};
     int run_first = t_begin, run_count = 0;
     for (int tile = t_begin; tile < t_end; ++tile) {
         int next = tile + 1 < t_end ? tile + 1 : A.ntiles;  // A.ntiles: none
         const int inst = g.inst;
-        const bool skip = g.skip;
-        const double dt = skip ? 0.0 : A.insts[inst].st->dt;
-        if (!skip) {
-            mixed_tile<MODEL, DIR, TS, NA>(A, g, h, l, neg, next, msm, racc);
+        TileGeom gn;
+        gn.inst = -1;
+        gn.skip = true;
+        if (!g.skip) {
+            mixed_tile<MODEL, DIR, TS, NA>(A, g, next, msm, racc, s_next, s_coef);
             ++run_count;
+            gn = s_next;
         } else if (next < A.ntiles) {
-            TileGeom gn = tile_geom<DIR, TS, NA>(A, next);
-            if (!gn.skip) tile_fetch<MODEL, DIR, TS, NA>(A, gn, h, l, neg);
+            gn = tile_geom<DIR, TS, NA>(A, next);
+            if (!gn.skip) tile_issue<MODEL, DIR, TS, NA>(A, gn, msm);
         }
-        bool run_ends = next >= A.ntiles || A.tile_inst[next] != inst;
+        bool run_ends = next >= A.ntiles || gn.inst != inst;
         if (DIR == DIR_Y && run_ends && run_count > 0) {
-            int t0 = run_first - A.tile_local[run_first];  // first tile of the instance
+            int t0 = run_first - A.tiles[run_first].local;  // first tile of the instance
             int c0 = t0 / A.chunk;
             int nslots = (t0 + A.insts[inst].tiles_y - 1) / A.chunk - c0 + 1;
-            flush_run(A, inst, (int)blockIdx.x - c0, nslots, run_count, racc, dt);
+            flush_run(A, inst, (int)blockIdx.x - c0, nslots, run_count, racc,
+                      A.insts[inst].st->dt);
         }
         if (run_ends) {
             run_count = 0;
             run_first = next;
         }
-        if (next < A.ntiles) g = tile_geom<DIR, TS, NA>(A, next);
+        g = gn;
         __syncthreads();  // shared memory is reused by the next tile
     }
+    cp_async_wait_all();
 }
 
 }  // namespace mixed
