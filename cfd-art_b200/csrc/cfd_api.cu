@@ -8,6 +8,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <utility>
@@ -18,6 +20,7 @@
 #include "cfd_error.h"
 #include "cfd_frame.h"
 #include "cfd_ic.h"
+#include "cfd_pool.h"
 #include "cfd_sweep.cuh"
 #include "ic_builders.h"
 
@@ -26,6 +29,42 @@ using namespace cfd;
 namespace {
 thread_local std::string g_err;
 }
+
+namespace cfd {
+
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t stream) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e) return e;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = pools.find(dev);
+        if (it == pools.end()) {
+            cudaMemPoolProps props;
+            memset(&props, 0, sizeof props);
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            if ((e = cudaMemPoolCreate(&pool, &props))) return e;
+            unsigned long long keep = ~0ULL;  // keep released blocks for reuse
+            if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)))
+                return e;
+            pools[dev] = pool;
+        } else {
+            pool = it->second;
+        }
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, stream);
+}
+
+cudaError_t pool_free(void* p, cudaStream_t stream) {
+    return p ? cudaFreeAsync(p, stream) : cudaSuccess;
+}
+
+}  // namespace cfd
 
 // Records the message cfd_last_error() returns on this thread.
 int cfd_fail(int code, const char* fmt, ...) {
@@ -580,16 +619,6 @@ int cfd_create(const cfd_config* cfg, cfd_solver** out) {
         return code;
     };
     cudaError_t e;
-    for (int b = 0; b < 2; ++b) {
-        e = cudaMalloc(&s->buf[b], s->buf_elems * sizeof(double));
-        if (e != cudaSuccess)
-            return cleanup(fail(CFD_ERR_NOMEM, "device allocation of %zu bytes failed: %s",
-                                s->buf_elems * sizeof(double), cudaGetErrorString(e)));
-    }
-    if ((e = cudaMalloc(&s->dst, sizeof(DevState))) != cudaSuccess ||
-        (e = cudaMalloc(&s->partials, 4 * sizeof(double) * s->max_blocks)) != cudaSuccess ||
-        (e = cudaMalloc(&s->counters, CNT_N * sizeof(unsigned long long))) != cudaSuccess)
-        return cleanup(fail(CFD_ERR_NOMEM, "device allocation failed: %s", cudaGetErrorString(e)));
     if (cfg->stream) {
         s->stream = (cudaStream_t)cfg->stream;
     } else {
@@ -597,6 +626,21 @@ int cfd_create(const cfd_config* cfg, cfd_solver** out) {
             return cleanup(fail(CFD_ERR_CUDA, "stream creation failed: %s", cudaGetErrorString(e)));
         s->own_stream = true;
     }
+    // stream-ordered allocations: no device-wide synchronisation while other
+    // solves run (a server creates and destroys solves between their rounds)
+    auto alloc = [&](void** p, size_t bytes) { return pool_alloc(p, bytes, s->stream); };
+    for (int b = 0; b < 2; ++b) {
+        e = alloc(reinterpret_cast<void**>(&s->buf[b]), s->buf_elems * sizeof(double));
+        if (e != cudaSuccess)
+            return cleanup(fail(CFD_ERR_NOMEM, "device allocation of %zu bytes failed: %s",
+                                s->buf_elems * sizeof(double), cudaGetErrorString(e)));
+    }
+    if ((e = alloc(reinterpret_cast<void**>(&s->dst), sizeof(DevState))) != cudaSuccess ||
+        (e = alloc(reinterpret_cast<void**>(&s->partials), 4 * sizeof(double) * s->max_blocks)) !=
+            cudaSuccess ||
+        (e = alloc(reinterpret_cast<void**>(&s->counters), CNT_N * sizeof(unsigned long long))) !=
+            cudaSuccess)
+        return cleanup(fail(CFD_ERR_NOMEM, "device allocation failed: %s", cudaGetErrorString(e)));
     DevState init;
     memset(&init, 0, sizeof init);
     init.T = cfg->T;
@@ -606,8 +650,7 @@ int cfd_create(const cfd_config* cfg, cfd_solver** out) {
     if ((e = cudaMemcpyAsync(s->dst, &init, sizeof init, cudaMemcpyHostToDevice, s->stream)) !=
             cudaSuccess ||
         (e = cudaMemsetAsync(s->counters, 0, CNT_N * sizeof(unsigned long long), s->stream)) !=
-            cudaSuccess ||
-        (e = cudaStreamSynchronize(s->stream)) != cudaSuccess)
+            cudaSuccess)
         return cleanup(fail(CFD_ERR_CUDA, "initialisation failed: %s", cudaGetErrorString(e)));
     *out = s;
     return CFD_OK;
@@ -622,12 +665,14 @@ int cfd_destroy(cfd_solver* s) {
             cudaEventDestroy(pr.first);
             cudaEventDestroy(pr.second);
         }
-    cudaFree(s->buf[0]);
-    cudaFree(s->buf[1]);
-    cudaFree(s->dst);
-    cudaFree(s->partials);
-    cudaFree(s->counters);
-    cudaFree(s->frame);
+    if (s->stream) {
+        pool_free(s->buf[0], s->stream);
+        pool_free(s->buf[1], s->stream);
+        pool_free(s->dst, s->stream);
+        pool_free(s->partials, s->stream);
+        pool_free(s->counters, s->stream);
+    }
+    if (s->frame) cudaFree(s->frame);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return CFD_OK;

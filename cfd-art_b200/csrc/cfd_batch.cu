@@ -28,6 +28,7 @@
 #include "cfd_error.h"
 #include "cfd_ic.h"
 #include "cfd_mixed.cuh"
+#include "cfd_pool.h"
 #include "ic_builders.h"
 
 using namespace cfd;
@@ -150,10 +151,11 @@ __global__ void soa_to_mixed(const double* __restrict__ soa, Inst I) {
     }
 }
 
-// Packed planes of buffer `buf` -> FP64 AoS with the boundary mirror in the
-// ghost strips (g = 0: interior only); corners are zero.
+// Packed planes of buffer `buf` (< 0: the current one) -> FP64 AoS with the
+// boundary mirror in the ghost strips (g = 0: interior only); corners are zero.
 __global__ void mixed_to_ghosted(Inst I, int buf, double* __restrict__ dst, int g, int im,
                                  int it, int use_bc) {
+    if (buf < 0) buf = I.st->cur & 1;  // the current buffer
     const int nx = I.nx, ny = I.ny, nv = I.nv;
     int W = nx + 2 * g, H = ny + 2 * g;
     long long n = (long long)W * H;
@@ -243,7 +245,23 @@ __global__ void init_reduce(const double* __restrict__ in, long long plane, int 
 
 constexpr int kInitBlocks = 148 * 2;
 
+struct PollRec {
+    double t;
+    int n, done;
+};
+
+// Time state of every member into one array (one copy to the host).
+__global__ void gather_status(const Inst* __restrict__ insts, int n, PollRec* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const DevState* st = insts[i].st;
+    out[i].t = st->t;
+    out[i].n = st->n;
+    out[i].done = st->done || st->n >= insts[i].max_steps;
+}
+
 struct Member {
+    bool final = false;   // seen done: later sweeps leave its state alone
     int id;
     cfd_config cfg;
     Inst inst;          // host copy of the device descriptor
@@ -278,11 +296,39 @@ struct cfd_batch {
     // autotuning state
     bool tuned = false;
     int tune_override = -1;
+    // uploads run on their own stream; batch-stream work waits for them
+    cudaStream_t copy = nullptr;
+    std::vector<cudaEvent_t> pending;
+    // status of every member gathered on the device, read with one copy
+    PollRec* d_poll = nullptr;
+    PollRec* h_poll = nullptr;  // pinned
+    int poll_cap = 0;
+    // asynchronous status gather of cfd_batch_step (finished members leave
+    // the tile lists without the host waiting for them)
+    PollRec* d_async = nullptr;
+    PollRec* h_async = nullptr;  // pinned
+    int async_cap = 0;
+    cudaEvent_t async_ev = nullptr;
+    bool async_pending = false;
+    std::vector<int> async_ids;  // member ids of the gathered entries
 };
 
 namespace {
 
+// Orders the batch stream after every upload queued on the copy stream.
+int wait_uploads(cfd_batch* b) {
+    cudaError_t r = cudaSuccess;
+    for (cudaEvent_t e : b->pending) {
+        if (r == cudaSuccess) r = cudaStreamWaitEvent(b->stream, e, 0);
+        cudaEventDestroy(e);  // its resources go once it has completed
+    }
+    b->pending.clear();
+    return r == cudaSuccess ? CFD_OK
+                            : cfd_fail(CFD_ERR_CUDA, "upload wait: %s", cudaGetErrorString(r));
+}
+
 int build_tables(cfd_batch* b) {
+    if (int r = wait_uploads(b)) return r;
     if (!b->dirty) return CFD_OK;
     b->groups.clear();
     std::vector<Inst> insts(b->members.size());
@@ -312,7 +358,7 @@ int build_tables(cfd_batch* b) {
             const Shape sh = dir == DIR_X ? kShapesX[g.shape] : kShapesY[g.shape];
             for (int idx : order) {
                 const Member& m = b->members[idx];
-                if (m.cfg.model != model) continue;
+                if (m.cfg.model != model || m.final) continue;  // finished: no tiles
                 const int len = dir == DIR_X ? m.cfg.nx : m.cfg.ny;
                 const int wid = dir == DIR_X ? m.cfg.ny : m.cfg.nx;
                 const int along = (len + sh.ts - 1) / sh.ts;
@@ -334,17 +380,17 @@ int build_tables(cfd_batch* b) {
             if (g.ntiles) b->groups.push_back(g);
         }
     if ((int)insts.size() > b->d_insts_cap) {
-        cudaFree(b->d_insts);
+        pool_free(b->d_insts, b->stream);
         b->d_insts = nullptr;
         int cap = std::max<int>(16, (int)insts.size() * 2);
-        BTRY(cudaMalloc(&b->d_insts, sizeof(Inst) * cap));
+        BTRY(pool_alloc(reinterpret_cast<void**>(&b->d_insts), sizeof(Inst) * cap, b->stream));
         b->d_insts_cap = cap;
     }
     if (all.size() > b->d_tiles_cap) {
-        cudaFree(b->d_tiles);
+        pool_free(b->d_tiles, b->stream);
         b->d_tiles = nullptr;
         size_t cap = std::max<size_t>(1024, all.size() * 2);
-        BTRY(cudaMalloc(&b->d_tiles, sizeof(TileEnt) * cap));
+        BTRY(pool_alloc(reinterpret_cast<void**>(&b->d_tiles), sizeof(TileEnt) * cap, b->stream));
         b->d_tiles_cap = cap;
     }
     if (!insts.empty())
@@ -353,7 +399,7 @@ int build_tables(cfd_batch* b) {
     if (!all.empty())
         BTRY(cudaMemcpyAsync(b->d_tiles, all.data(), sizeof(TileEnt) * all.size(),
                              cudaMemcpyHostToDevice, b->stream));
-    BTRY(cudaStreamSynchronize(b->stream));  // host vectors die at return
+    // pageable sources: the host vectors have been read when the copy calls return
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -433,6 +479,11 @@ int cfd_batch_create(void* stream, size_t device_budget_bytes, cfd_batch** out) 
         }
         b->own_stream = true;
     }
+    if (cudaStreamCreateWithFlags(&b->copy, cudaStreamNonBlocking) != cudaSuccess) {
+        if (b->own_stream) cudaStreamDestroy(b->stream);
+        delete b;
+        return cfd_fail(CFD_ERR_CUDA, "copy stream creation failed");
+    }
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
@@ -448,11 +499,21 @@ int cfd_batch_create(void* stream, size_t device_budget_bytes, cfd_batch** out) 
 
 int cfd_batch_destroy(cfd_batch* b) {
     if (!b) return CFD_OK;
+    cudaStreamSynchronize(b->copy);
+    for (cudaEvent_t e : b->pending) cudaEventDestroy(e);
+    b->pending.clear();
     cudaStreamSynchronize(b->stream);
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    for (auto& m : b->members) cudaFree(m.mem);
-    cudaFree(b->d_insts);
-    cudaFree(b->d_tiles);
+    for (auto& m : b->members) pool_free(m.mem, b->stream);
+    pool_free(b->d_insts, b->stream);
+    pool_free(b->d_tiles, b->stream);
+    pool_free(b->d_poll, b->stream);
+    pool_free(b->d_async, b->stream);
+    cudaStreamSynchronize(b->stream);
+    if (b->h_poll) cudaFreeHost(b->h_poll);
+    if (b->h_async) cudaFreeHost(b->h_async);
+    if (b->async_ev) cudaEventDestroy(b->async_ev);
+    cudaStreamDestroy(b->copy);
     if (b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
     return CFD_OK;
@@ -464,8 +525,6 @@ int cfd_batch_member_bytes(const cfd_config* cfg, size_t* bytes) {
     return CFD_OK;
 }
 
-// Adds a member whose initial state is either a ghosted AoS host grid or a
-// shape program built on the device.
 // Saved state of a member (cfd_batch_restore): packed value and
 // compensation planes (nx * ny cells each, no padding) and its time state.
 struct Restore {
@@ -473,6 +532,11 @@ struct Restore {
     const float4* q4[2];
     const float2* q2[2];
 };
+
+// Adds a member whose initial state is either a ghosted AoS host grid or a
+// shape program built on the device.  The upload runs on the batch's copy
+// stream, so it overlaps sweeps already queued; the next batch operation
+// waits for it.
 
 static int add_member(cfd_batch* b, const cfd_config* cfg, const double* host_ic,
                       const std::vector<cfdic::Op>* prog, const cfdic::Eos* prog_eos,
@@ -497,7 +561,7 @@ static int add_member(cfd_batch* b, const cfd_config* cfg, const double* host_ic
     m.cfg = c;
     m.max_steps = max_steps;
     m.bytes = bytes;
-    BTRY(cudaMalloc(&m.mem, bytes));
+    BTRY(pool_alloc(&m.mem, bytes, b->copy));
     int nv = cfd_nvar(c.model);
     char* p = static_cast<char*>(m.mem);
     auto take = [&](size_t n) {
@@ -564,9 +628,11 @@ static int add_member(cfd_batch* b, const cfd_config* cfg, const double* host_ic
     size_t ghosted = host_ic ? (size_t)nv * (c.nx + 2 * g) * (size_t)(c.ny + 2 * g) : 0;
     size_t soa = rs ? 0 : (size_t)nv * plane;
     double* staging = nullptr;
-    cudaError_t e = rs ? cudaSuccess : cudaMalloc(&staging, sizeof(double) * (ghosted + soa));
+    cudaError_t e = rs ? cudaSuccess
+                       : pool_alloc(reinterpret_cast<void**>(&staging),
+                                    sizeof(double) * (ghosted + soa), b->copy);
     if (e != cudaSuccess) {
-        cudaFree(m.mem);
+        pool_free(m.mem, b->copy);
         return cfd_fail(CFD_ERR_NOMEM, "staging: %s", cudaGetErrorString(e));
     }
     DevState init;
@@ -591,52 +657,61 @@ static int add_member(cfd_batch* b, const cfd_config* cfg, const double* host_ic
             for (int w = 0; w < 2 && !e; ++w) {
                 e = cudaMemcpy2DAsync(I.q4[0][w], pitch * sizeof(float4), rs->q4[w],
                                       c.nx * sizeof(float4), c.nx * sizeof(float4), c.ny,
-                                      cudaMemcpyHostToDevice, b->stream);
+                                      cudaMemcpyHostToDevice, b->copy);
                 if (!e && nv == 6)
                     e = cudaMemcpy2DAsync(I.q2[0][w], pitch * sizeof(float2), rs->q2[w],
                                           c.nx * sizeof(float2), c.nx * sizeof(float2), c.ny,
-                                          cudaMemcpyHostToDevice, b->stream);
+                                          cudaMemcpyHostToDevice, b->copy);
             }
-            if (!e) e = cudaMemcpyAsync(I.st, &init, sizeof init, cudaMemcpyHostToDevice, b->stream);
-            if (!e) e = cudaStreamSynchronize(b->stream);
+            if (!e) e = cudaMemcpyAsync(I.st, &init, sizeof init, cudaMemcpyHostToDevice, b->copy);
+            if (!e) e = cudaStreamSynchronize(b->copy);
             if (e) r = cfd_fail(CFD_ERR_CUDA, "restore: %s", cudaGetErrorString(e));
             break;
         }
-        if ((e = cudaMemcpyAsync(I.st, &init, sizeof init, cudaMemcpyHostToDevice, b->stream))) {
+        if ((e = cudaMemcpyAsync(I.st, &init, sizeof init, cudaMemcpyHostToDevice, b->copy))) {
             r = cfd_fail(CFD_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
             break;
         }
         if (host_ic) {
             if ((e = cudaMemcpyAsync(staging, host_ic, sizeof(double) * ghosted,
-                                     cudaMemcpyHostToDevice, b->stream))) {
+                                     cudaMemcpyHostToDevice, b->copy))) {
                 r = cfd_fail(CFD_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
                 break;
             }
-            ghosted_to_mixed<<<148 * 4, 256, 0, b->stream>>>(staging, I, staging + ghosted, g);
+            ghosted_to_mixed<<<148 * 4, 256, 0, b->copy>>>(staging, I, staging + ghosted, g);
         } else {
             cfdic::Geom geo{c.x0, c.y0, c.dx, c.dy};
             if ((e = cfdic::build_device(*prog, *prog_eos, geo, c.nx, c.ny, staging,
-                                         (long long)plane, pitch, b->stream))) {
+                                         (long long)plane, pitch, b->copy))) {
                 r = cfd_fail(CFD_ERR_CUDA, "initial condition: %s", cudaGetErrorString(e));
                 break;
             }
-            soa_to_mixed<<<148 * 4, 256, 0, b->stream>>>(staging, I);
+            soa_to_mixed<<<148 * 4, 256, 0, b->copy>>>(staging, I);
         }
         if (c.model == CFD_MODEL_EULER)
-            init_reduce<MODEL_EULER><<<kInitBlocks, 256, 0, b->stream>>>(
+            init_reduce<MODEL_EULER><<<kInitBlocks, 256, 0, b->copy>>>(
                 staging + ghosted, (long long)plane, pitch, c.nx, c.ny, I.eos, I.st, I.partials);
         else
-            init_reduce<MODEL_ALLAIRE><<<kInitBlocks, 256, 0, b->stream>>>(
+            init_reduce<MODEL_ALLAIRE><<<kInitBlocks, 256, 0, b->copy>>>(
                 staging + ghosted, (long long)plane, pitch, c.nx, c.ny, I.eos, I.st, I.partials);
-        if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(b->stream))) {
+        // no synchronisation: the pageable source has been read when the copy
+        // call returns, and everything else is ordered on the batch stream
+        if ((e = cudaGetLastError())) {
             r = cfd_fail(CFD_ERR_CUDA, "upload kernels: %s", cudaGetErrorString(e));
             break;
         }
     } while (0);
-    cudaFree(staging);
+    pool_free(staging, b->copy);
     if (r) {
-        cudaFree(m.mem);
+        pool_free(m.mem, b->copy);
         return r;
+    }
+    cudaEvent_t done_ev;
+    if (cudaEventCreateWithFlags(&done_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventRecord(done_ev, b->copy) != cudaSuccess) {
+        cudaStreamSynchronize(b->copy);  // fall back to waiting here
+    } else {
+        b->pending.push_back(done_ev);
     }
     b->used += bytes;
     b->members.push_back(m);
@@ -669,10 +744,10 @@ static Member* find(cfd_batch* b, int id) {
 
 int cfd_batch_remove(cfd_batch* b, int id) {
     if (!b) return cfd_fail(CFD_ERR_INVALID, "null batch");
+    if (int r = wait_uploads(b)) return r;
     for (size_t i = 0; i < b->members.size(); ++i)
         if (b->members[i].id == id) {
-            BTRY(cudaStreamSynchronize(b->stream));
-            cudaFree(b->members[i].mem);
+            pool_free(b->members[i].mem, b->stream);  // after the work queued so far
             b->used -= b->members[i].bytes;
             b->members.erase(b->members.begin() + i);
             b->dirty = true;
@@ -758,30 +833,84 @@ int cfd_batch_autotune(cfd_batch* b, int steps_per_trial, double* best_ms) {
     return build_tables(b);
 }
 
+// Reads a completed asynchronous status gather (never waits) and takes the
+// members it found done out of the tile lists.
+static void take_async_status(cfd_batch* b) {
+    if (!b->async_pending || cudaEventQuery(b->async_ev) != cudaSuccess) return;
+    b->async_pending = false;
+    for (size_t i = 0; i < b->async_ids.size(); ++i) {
+        if (!b->h_async[i].done) continue;
+        Member* m = find(b, b->async_ids[i]);
+        if (m && !m->final) {
+            m->final = true;
+            b->dirty = true;
+        }
+    }
+}
+
+// Queues a status gather of every member and its copy to pinned memory.
+static int issue_async_status(cfd_batch* b) {
+    const int n = (int)b->members.size();
+    if (b->async_pending || n == 0) return CFD_OK;
+    if (!b->async_ev) BTRY(cudaEventCreateWithFlags(&b->async_ev, cudaEventDisableTiming));
+    if (n > b->async_cap) {
+        pool_free(b->d_async, b->stream);
+        b->d_async = nullptr;
+        if (b->h_async) {
+            BTRY(cudaStreamSynchronize(b->stream));
+            cudaFreeHost(b->h_async);
+            b->h_async = nullptr;
+        }
+        int c = std::max(64, 2 * n);
+        BTRY(pool_alloc(reinterpret_cast<void**>(&b->d_async), sizeof(PollRec) * c, b->stream));
+        BTRY(cudaHostAlloc(reinterpret_cast<void**>(&b->h_async), sizeof(PollRec) * c,
+                           cudaHostAllocDefault));
+        b->async_cap = c;
+    }
+    gather_status<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_insts, n, b->d_async);
+    BTRY(cudaGetLastError());
+    BTRY(cudaMemcpyAsync(b->h_async, b->d_async, sizeof(PollRec) * n, cudaMemcpyDeviceToHost,
+                         b->stream));
+    BTRY(cudaEventRecord(b->async_ev, b->stream));
+    b->async_ids.resize(n);
+    for (int i = 0; i < n; ++i) b->async_ids[i] = b->members[i].id;
+    b->async_pending = true;
+    return CFD_OK;
+}
+
 int cfd_batch_step(cfd_batch* b, int ticks) {
     if (!b) return cfd_fail(CFD_ERR_INVALID, "null batch");
     if (ticks <= 0 || b->members.empty()) return CFD_OK;
-    int r = build_tables(b);
-    if (r) return r;
-    const int K = 8;
-    if (ticks >= K) {
-        if (!b->graph) {
-            BTRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            int rr = CFD_OK;
-            for (int i = 0; i < K && rr == CFD_OK; ++i) rr = enqueue_tick(b, nullptr);
-            cudaGraph_t gph;
-            cudaError_t e = cudaStreamEndCapture(b->stream, &gph);
-            if (rr) return rr;
-            if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "capture: %s", cudaGetErrorString(e));
-            e = cudaGraphInstantiate(&b->graph, gph, 0);
-            cudaGraphDestroy(gph);
-            if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
-            b->graph_steps = K;
+    const int K = 8;            // ticks per captured graph
+    const int kCheck = 64;      // ticks between status gathers
+    int r;
+    for (int done_ticks = 0; done_ticks < ticks;) {
+        take_async_status(b);
+        if ((r = build_tables(b))) return r;
+        if (b->groups.empty()) break;  // every member has finished
+        const int chunk = std::min(kCheck, ticks - done_ticks);
+        if (chunk >= K) {
+            if (!b->graph) {
+                BTRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+                int rr = CFD_OK;
+                for (int i = 0; i < K && rr == CFD_OK; ++i) rr = enqueue_tick(b, nullptr);
+                cudaGraph_t gph;
+                cudaError_t e = cudaStreamEndCapture(b->stream, &gph);
+                if (rr) return rr;
+                if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "capture: %s", cudaGetErrorString(e));
+                e = cudaGraphInstantiate(&b->graph, gph, 0);
+                cudaGraphDestroy(gph);
+                if (e != cudaSuccess)
+                    return cfd_fail(CFD_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
+                b->graph_steps = K;
+            }
+            for (int i = 0; i + K <= chunk; i += K) BTRY(cudaGraphLaunch(b->graph, b->stream));
         }
-        for (int i = 0; i + K <= ticks; i += K) BTRY(cudaGraphLaunch(b->graph, b->stream));
+        for (int i = 0; i < chunk % K; ++i)
+            if ((r = enqueue_tick(b, nullptr))) return r;
+        done_ticks += chunk;
+        if (done_ticks < ticks && (r = issue_async_status(b))) return r;
     }
-    for (int i = 0; i < ticks % K; ++i)
-        if ((r = enqueue_tick(b, nullptr))) return r;
     return CFD_OK;
 }
 
@@ -812,12 +941,14 @@ int cfd_batch_status(cfd_batch* b, int id, cfd_status* out) {
     if (!b || !out) return cfd_fail(CFD_ERR_INVALID, "null argument");
     Member* m = find(b, id);
     if (!m) return cfd_fail(CFD_ERR_INVALID, "no instance %d", id);
+    if (int r = wait_uploads(b)) return r;
     DevState d;
     BTRY(cudaMemcpyAsync(&d, m->inst.st, sizeof d, cudaMemcpyDeviceToHost, b->stream));
     BTRY(cudaStreamSynchronize(b->stream));
     memset(out, 0, sizeof *out);
     out->n = d.n;
     out->done = d.done || d.n >= m->max_steps;
+    if (out->done) m->final = true;
     out->t = d.t;
     out->dt_next = d.dt;
     out->maxu = d.maxu;
@@ -833,16 +964,34 @@ int cfd_batch_poll(cfd_batch* b, int cap, int* ids, int* steps, int* done, doubl
     if (!b || !count) return cfd_fail(CFD_ERR_INVALID, "null argument");
     int n = (int)b->members.size();
     *count = n;
-    std::vector<DevState> ds(n);
-    for (int i = 0; i < n; ++i)
-        BTRY(cudaMemcpyAsync(&ds[i], b->members[i].inst.st, sizeof(DevState),
-                             cudaMemcpyDeviceToHost, b->stream));
+    if (n == 0) return CFD_OK;
+    int r = build_tables(b);  // the device descriptor array follows the membership
+    if (r) return r;
+    if (n > b->poll_cap) {
+        pool_free(b->d_poll, b->stream);
+        b->d_poll = nullptr;
+        if (b->h_poll) {
+            BTRY(cudaStreamSynchronize(b->stream));
+            cudaFreeHost(b->h_poll);
+            b->h_poll = nullptr;
+        }
+        int c = std::max(64, 2 * n);
+        BTRY(pool_alloc(reinterpret_cast<void**>(&b->d_poll), sizeof(PollRec) * c, b->stream));
+        BTRY(cudaHostAlloc(reinterpret_cast<void**>(&b->h_poll), sizeof(PollRec) * c,
+                           cudaHostAllocDefault));
+        b->poll_cap = c;
+    }
+    gather_status<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_insts, n, b->d_poll);
+    BTRY(cudaGetLastError());
+    BTRY(cudaMemcpyAsync(b->h_poll, b->d_poll, sizeof(PollRec) * n, cudaMemcpyDeviceToHost,
+                         b->stream));
     BTRY(cudaStreamSynchronize(b->stream));
     for (int i = 0; i < n && i < cap; ++i) {
         if (ids) ids[i] = b->members[i].id;
-        if (steps) steps[i] = ds[i].n;
-        if (done) done[i] = ds[i].done || ds[i].n >= b->members[i].max_steps;
-        if (t) t[i] = ds[i].t;
+        if (steps) steps[i] = b->h_poll[i].n;
+        if (done) done[i] = b->h_poll[i].done;
+        if (b->h_poll[i].done) b->members[i].final = true;
+        if (t) t[i] = b->h_poll[i].t;
     }
     return CFD_OK;
 }
@@ -851,6 +1000,7 @@ int cfd_batch_save(cfd_batch* b, int id, const char* path) {
     if (!b || !path) return cfd_fail(CFD_ERR_INVALID, "null argument");
     Member* m = find(b, id);
     if (!m) return cfd_fail(CFD_ERR_INVALID, "no instance %d", id);
+    if (int r = wait_uploads(b)) return r;
     const cfd_config& c = m->cfg;
     const Inst& I = m->inst;
     DevState d;
@@ -959,26 +1109,35 @@ int cfd_batch_download(cfd_batch* b, int id, double* host, int layout) {
     Member* m = find(b, id);
     if (!m) return cfd_fail(CFD_ERR_INVALID, "no instance %d", id);
     const cfd_config& c = m->cfg;
-    DevState d;
-    BTRY(cudaMemcpyAsync(&d, m->inst.st, sizeof d, cudaMemcpyDeviceToHost, b->stream));
-    BTRY(cudaStreamSynchronize(b->stream));
-    int cur = d.cur & 1;
+    // On the copy stream: a member seen done is no longer written by the
+    // sweeps, so its copy overlaps them; otherwise it waits for the work
+    // queued on the batch stream so far.
+    if (int r = wait_uploads(b)) return r;
+    if (!m->final) {
+        cudaEvent_t ev;
+        BTRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaError_t e = cudaEventRecord(ev, b->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->copy, ev, 0);
+        cudaEventDestroy(ev);
+        if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "download: %s", cudaGetErrorString(e));
+    }
+    const int cur = -1;  // read on the device
     int nv = cfd_nvar(c.model), g = c.flux_solver == CFD_FLUX_GODUNOV ? 1 : 2;
     size_t elems = layout == CFD_LAYOUT_GHOSTED_AOS
                        ? (size_t)nv * (c.nx + 2 * g) * (size_t)(c.ny + 2 * g)
                        : (size_t)nv * c.nx * c.ny;
     double* tmp = nullptr;
-    BTRY(cudaMalloc(&tmp, sizeof(double) * elems));
+    BTRY(pool_alloc(reinterpret_cast<void**>(&tmp), sizeof(double) * elems, b->copy));
     int im = c.model == CFD_MODEL_EULER ? 1 : 2;
     if (layout == CFD_LAYOUT_GHOSTED_AOS)
-        mixed_to_ghosted<<<148 * 4, 256, 0, b->stream>>>(m->inst, cur, tmp, g, im, im + 1, 1);
+        mixed_to_ghosted<<<148 * 4, 256, 0, b->copy>>>(m->inst, cur, tmp, g, im, im + 1, 1);
     else  // interior only, AoS; reordered to SoA planes below
-        mixed_to_ghosted<<<148 * 4, 256, 0, b->stream>>>(m->inst, cur, tmp, 0, -1, -1, 0);
+        mixed_to_ghosted<<<148 * 4, 256, 0, b->copy>>>(m->inst, cur, tmp, 0, -1, -1, 0);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(host, tmp, sizeof(double) * elems, cudaMemcpyDeviceToHost, b->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-    cudaFree(tmp);
+        e = cudaMemcpyAsync(host, tmp, sizeof(double) * elems, cudaMemcpyDeviceToHost, b->copy);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->copy);
+    pool_free(tmp, b->copy);
     if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "download: %s", cudaGetErrorString(e));
     if (layout == CFD_LAYOUT_SOA) {
         // the kernel wrote AoS interior; reorder to SoA planes on the host

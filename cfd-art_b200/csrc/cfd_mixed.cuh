@@ -764,8 +764,11 @@ __device__ __forceinline__ void flush_run(const MixedArgs& A, int inst, int slot
 // Persistent sweep: a fixed grid of CTAs walks the tile list of every
 // instance in the launch; each thread loads its cell of the next tile while
 // the current tile is being computed.
+// Resident CTAs per SM: 4 for the Euler x sweep, 3 where the register need
+// is larger (the Euler y sweep with its reduction, every Allaire sweep).
 template <int MODEL, int DIR, int TS, int NA>
-__global__ void __launch_bounds__(256, MODEL == MODEL_EULER ? 4 : 3) mixed_sweep_kernel(MixedArgs A) {
+__global__ void __launch_bounds__(256, (MODEL == MODEL_EULER && DIR == DIR_X) ? 4 : 3)
+    mixed_sweep_kernel(MixedArgs A) {
     extern __shared__ __align__(16) char msm[];
     __shared__ TileGeom s_next;
     __shared__ float s_coef[2];

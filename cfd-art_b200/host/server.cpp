@@ -15,6 +15,7 @@
 // process, euler_equations/euler_simulation_code/sourcecode/main.cpp:17-49).
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -51,6 +52,8 @@ struct Request {
     Clock::time_point t_submit, t_admit, t_done;
     int member = -1;          // batch member id (mixed)
     cfd_solver* solver = nullptr;  // FP64
+    cudaStream_t stream = nullptr; // FP64: the solve's own stream
+    cudaEvent_t ev = nullptr;      // FP64: end of its part of a round
     int issued = 0;                // FP64: steps enqueued so far
     size_t bytes = 0;
     cfd_status final_status{};
@@ -125,29 +128,65 @@ void finish(cfd_server* s, Request* r, int err) {
     }
 }
 
+// Returns a finished request's grid to it and releases its device state.
+int collect(cfd_server* s, Request* r) {
+    if (r->ic.empty()) {  // device-built initial condition: room for the result
+        size_t elems = 0;
+        cfd_ic_grid_elems(&r->cfg, &elems);
+        r->ic.resize(elems);
+    }
+    int rc;
+    if (s->opt.precision == CFD_PREC_MIXED) {
+        rc = cfd_batch_download(s->batch, r->member, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS);
+        cfd_batch_remove(s->batch, r->member);
+    } else {
+        rc = cfd_download(r->solver, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS);
+        cfd_destroy(r->solver);
+        r->solver = nullptr;
+        cudaStreamDestroy(r->stream);
+        r->stream = nullptr;
+        cudaEventDestroy(r->ev);
+        r->ev = nullptr;
+    }
+    return rc;
+}
+
+// The worker: admission, one round of steps for every admitted solve, then
+// completion.  Host work overlaps the round in flight: uploads of admitted
+// solves run on their own streams (the batch's copy stream, or each FP64
+// solve's stream), and the grids of solves found finished by the previous
+// round's status read are copied back while the next round runs.
 void worker_main(cfd_server* s) {
     cudaSetDevice(s->device);
     const int K = std::max(1, s->opt.ticks_per_round);
+    const bool mixed = s->opt.precision == CFD_PREC_MIXED;
+    std::vector<Request*> finished;  // found done, grids not yet collected
     while (true) {
         std::vector<Request*> start;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty() || !s->running.empty(); });
+            s->cv_work.wait(lk, [&] {
+                return s->stop || !s->queue.empty() || !s->running.empty() || !finished.empty();
+            });
             if (s->stop) break;
             admit(s, start);
         }
-        // start admitted requests (device allocation + upload)
+        // start admitted requests (device allocation + upload, asynchronous)
         for (Request* r : start) {
             int rc;
-            if (s->opt.precision == CFD_PREC_MIXED) {
+            if (mixed) {
                 rc = r->recipe ? cfd_batch_add_recipe(s->batch, &r->cfg, r->recipe, r->seed,
                                                       r->nbubbles, r->steps, &r->member)
                                : cfd_batch_add(s->batch, &r->cfg, r->ic.data(), r->steps,
                                                &r->member);
             } else {
                 cfd_config c = r->cfg;
-                c.stream = s->stream;
-                rc = cfd_create(&c, &r->solver);
+                rc = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) == cudaSuccess &&
+                             cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) == cudaSuccess
+                         ? CFD_OK
+                         : CFD_ERR_CUDA;
+                c.stream = r->stream;
+                if (!rc) rc = cfd_create(&c, &r->solver);
                 if (!rc)
                     rc = r->recipe ? cfd_upload_recipe(r->solver, r->recipe, r->seed, r->nbubbles,
                                                        0, 0.0)
@@ -166,51 +205,78 @@ void worker_main(cfd_server* s) {
         std::vector<Request*> run;
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            for (int64_t id : s->running) run.push_back(s->reqs[id].get());
+            for (int64_t id : s->running) {
+                Request* r = s->reqs[id].get();
+                if (std::find(finished.begin(), finished.end(), r) == finished.end())
+                    run.push_back(r);
+            }
             s->max_running = std::max<int>(s->max_running, (int)run.size());
         }
-        if (run.empty()) continue;
         auto tr = Clock::now();
-        // one round of batched steps
-        cudaEventRecord(s->ev0, s->stream);
-        if (s->opt.precision == CFD_PREC_MIXED) {
-            if (cfd_batch_step(s->batch, K)) s->worker_error = CFD_ERR_CUDA;
-        } else {
-            for (Request* r : run) {
-                int k = std::min(K, r->steps - r->issued);
-                if (k > 0 && cfd_advance(r->solver, k) == CFD_OK) r->issued += k;
-            }
-        }
-        cudaEventRecord(s->ev1, s->stream);
-        // completion check: one status read per member
-        std::vector<Request*> done;
-        for (Request* r : run) {
-            cfd_status st;
-            int rc = s->opt.precision == CFD_PREC_MIXED ? cfd_batch_status(s->batch, r->member, &st)
-                                                         : cfd_get_status(r->solver, &st);
-            if (rc || st.done || st.n >= r->steps) {
-                r->final_status = st;
-                done.push_back(r);
-            }
-        }
-        for (Request* r : done) {
-            int rc;
-            if (r->ic.empty()) {  // device-built initial condition: room for the result
-                size_t elems = 0;
-                cfd_ic_grid_elems(&r->cfg, &elems);
-                r->ic.resize(elems);
-            }
-            if (s->opt.precision == CFD_PREC_MIXED) {
-                rc = cfd_batch_download(s->batch, r->member, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS);
-                cfd_batch_remove(s->batch, r->member);
+        // one round of steps (asynchronous)
+        if (!run.empty()) {
+            cudaEventRecord(s->ev0, s->stream);
+            if (mixed) {
+                if (cfd_batch_step(s->batch, K)) s->worker_error = CFD_ERR_CUDA;
             } else {
-                rc = cfd_download(r->solver, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS);
-                cfd_destroy(r->solver);
-                r->solver = nullptr;
+                for (Request* r : run) {
+                    cudaStreamWaitEvent(r->stream, s->ev0, 0);
+                    int k = std::min(K, r->steps - r->issued);
+                    if (k > 0 && cfd_advance(r->solver, k) == CFD_OK) r->issued += k;
+                    cudaEventRecord(r->ev, r->stream);
+                    cudaStreamWaitEvent(s->stream, r->ev, 0);
+                }
             }
+            cudaEventRecord(s->ev1, s->stream);
+        }
+        // grids of the solves the previous status read found finished, while
+        // the round runs
+        for (Request* r : finished) {
+            int rc = collect(s, r);
             std::lock_guard<std::mutex> lk(s->mu);
             s->running.erase(std::find(s->running.begin(), s->running.end(), r->id));
             finish(s, r, rc);
+        }
+        if (!finished.empty()) s->cv_done.notify_all();
+        finished.clear();
+        if (run.empty()) continue;
+        // completion check: mixed, one gathered status read for the whole
+        // batch; FP64, a status read only for solves that may have finished
+        // (all steps issued, or a finite end time)
+        if (mixed) {
+            int n = 0;
+            const int cap = (int)run.size() + 64;
+            std::vector<int> ids(cap), steps(cap), fin(cap);
+            std::vector<double> tt(cap);
+            int rc = cfd_batch_poll(s->batch, cap, ids.data(), steps.data(), fin.data(), tt.data(),
+                                    &n);
+            std::map<int, int> pos;
+            for (int i = 0; i < n && i < cap; ++i) pos[ids[i]] = i;
+            for (Request* r : run) {
+                auto it = pos.find(r->member);
+                if (rc || it == pos.end()) {
+                    finished.push_back(r);
+                    continue;
+                }
+                int i = it->second;
+                if (fin[i] || steps[i] >= r->steps) {
+                    memset(&r->final_status, 0, sizeof r->final_status);
+                    r->final_status.n = steps[i];
+                    r->final_status.t = tt[i];
+                    r->final_status.done = fin[i];
+                    finished.push_back(r);
+                }
+            }
+        } else {
+            for (Request* r : run) {
+                if (r->issued < r->steps && std::isinf(r->cfg.T)) continue;
+                cfd_status st;
+                int rc = cfd_get_status(r->solver, &st);
+                if (rc || st.done || st.n >= r->steps) {
+                    r->final_status = st;
+                    finished.push_back(r);
+                }
+            }
         }
         float dev_ms = 0.f;
         cudaEventSynchronize(s->ev1);
@@ -221,7 +287,6 @@ void worker_main(cfd_server* s) {
             s->device_s += 1e-3 * dev_ms;
             s->rounds++;
         }
-        if (!done.empty()) s->cv_done.notify_all();
     }
 }
 
@@ -380,8 +445,12 @@ int cfd_server_destroy(cfd_server* s) {
     }
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();
-    for (auto& kv : s->reqs)
-        if (kv.second->solver) cfd_destroy(kv.second->solver);
+    for (auto& kv : s->reqs) {
+        Request* r = kv.second.get();
+        if (r->solver) cfd_destroy(r->solver);
+        if (r->stream) cudaStreamDestroy(r->stream);
+        if (r->ev) cudaEventDestroy(r->ev);
+    }
     if (s->batch) cfd_batch_destroy(s->batch);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
