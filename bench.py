@@ -301,8 +301,12 @@ def run_reference(args) -> None:
 # ---------------------------------------------------------------- GPU arms --
 
 class Ctx:
-    def __init__(self, torch, dist, world, rank, local):
+    """Ranks of one job: barrier, and max / sum over ranks (one process per
+    GPU, NCCL; the tests run the same code on CPU ranks over gloo)."""
+
+    def __init__(self, torch, dist, world, rank, local, device="cuda"):
         self.torch, self.dist, self.world, self.rank, self.local = torch, dist, world, rank, local
+        self.device = device
 
     def barrier(self):
         if self.world > 1:
@@ -311,16 +315,22 @@ class Ctx:
     def max(self, x: float) -> float:
         if self.world == 1:
             return x
-        t = self.torch.tensor([x], device="cuda", dtype=self.torch.float64)
+        t = self.torch.tensor([x], device=self.device, dtype=self.torch.float64)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
     def sum(self, x: float) -> float:
         if self.world == 1:
             return x
-        t = self.torch.tensor([x], device="cuda", dtype=self.torch.float64)
+        t = self.torch.tensor([x], device=self.device, dtype=self.torch.float64)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
         return float(t.item())
+
+
+def job_throughput(ctx, cell_updates: float, ms: float) -> float:
+    """Whole-job Gcell-updates/s of N replicas: the updates of all ranks over
+    the slowest rank's device time."""
+    return ctx.sum(cell_updates) / (ctx.max(ms) / 1e3) / 1e9
 
 
 def roofline(kernel: str, ms: float, launches: int, bytes_per_launch: float, traffic_key: str):
@@ -385,7 +395,7 @@ def bench_single(args, ctx, G, stream, clocks):
     e2e = None
     if not args.no_e2e:
         e2e = e2e_single(G, torch, cfg, ic, K, W, ctx, prec)
-    value = ctx.world * cells * K / (ms / 1e3) / 1e9
+    value = job_throughput(ctx, cells * K, ms)
     config = {"workload": args.workload, "model": model, "precision": prec, "grid": [nx, ny],
               "bubbles": nbub, "seed": SEED, "cfl": cfg.cfl,
               "l2": f"state {cells * nv * 8 / 1e6:.0f} MB per buffer vs 126 MB L2"
@@ -461,7 +471,7 @@ def bench_batch(args, ctx, G, stream, clocks):
                   f"batch_mixed_sweep_{'xy'[dom]}")
     shapes = b.get_shapes(0)
     b.close()
-    value = ctx.sum(upd) / (ms / 1e3) / 1e9
+    value = job_throughput(ctx, upd, ms)
     e2e = None
     if not args.no_e2e:
         ctx.barrier()
@@ -550,7 +560,7 @@ def bench_served(args, ctx, G, stream, clocks):
     ck = clocks.stop()
     ms = ctx.max(e0.elapsed_time(e1))
     res_upd = sum(b.cfgs[i].nx * b.cfgs[i].ny * (r[4] - before[i]) for i, r in zip(ids, timed))
-    value = ctx.sum(res_upd) / (ms / 1e3) / 1e9
+    value = job_throughput(ctx, res_upd, ms)
     b.close()
     # roofline of the mixed sweeps on a resident sample (16 requests)
     b = G.Batch(stream=stream.cuda_stream)
