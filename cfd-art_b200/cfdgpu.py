@@ -503,10 +503,12 @@ class Batch:
         check(lib().cfd_batch_poll(self._h, n, ids, steps, done, t, C.byref(cnt)), "cfd_batch_poll")
         return [(ids[i], steps[i], bool(done[i]), t[i]) for i in range(cnt.value)]
 
-    def download(self, mid: int, layout: int = GHOSTED_AOS) -> np.ndarray:
+    def download(self, mid: int, layout: int = GHOSTED_AOS,
+                 out: np.ndarray | None = None) -> np.ndarray:
         c = self.cfgs[mid]
-        shape = c.ghosted_shape() if layout == GHOSTED_AOS else (c.nvar, c.ny, c.nx)
-        out = np.empty(shape)
+        if out is None:
+            shape = c.ghosted_shape() if layout == GHOSTED_AOS else (c.nvar, c.ny, c.nx)
+            out = np.empty(shape)
         check(lib().cfd_batch_download(self._h, mid, _dp(out), layout), "cfd_batch_download")
         return out
 
