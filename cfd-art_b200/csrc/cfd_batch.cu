@@ -27,6 +27,7 @@
 #include "cfd_checkpoint.h"
 #include "cfd_error.h"
 #include "cfd_ic.h"
+#include "cfd_march.cuh"
 #include "cfd_mixed.cuh"
 #include "cfd_pool.h"
 #include "ic_builders.h"
@@ -49,9 +50,13 @@ namespace {
 struct Shape {
     int ts, na;
 };
+// y shape 3: marching strips of 32 columns x kMarchRows rows (cfd_march.cuh);
+// in x the marching form (lanes on 32 different rows) measured 1.9x slower
+// than the tiles, so x keeps the three tile shapes
 constexpr Shape kShapesX[] = {{60, 4}, {124, 2}, {28, 8}};
-constexpr Shape kShapesY[] = {{28, 8}, {60, 4}, {12, 16}};
-constexpr int kNumShapes = 3;
+constexpr Shape kShapesY[] = {{28, 8}, {60, 4}, {12, 16}, {kMarchRows, 32}};
+constexpr int kNumShapesX = 3, kNumShapesY = 4;
+constexpr int kMarchShape = 3;
 
 // Persistent launch: as many CTAs as fit on the device at once (occupancy
 // of this variant), never more than there are tiles.
@@ -77,6 +82,26 @@ int launch_t(const MixedArgs& a, int sms, cudaStream_t st) {
     return CFD_OK;
 }
 
+// Persistent marching y sweep (4-warp CTAs): as many warps as fit on the device, each
+// walking a contiguous range of strips.
+template <int MODEL, int DIR>
+int launch_march(const MixedArgs& a, int sms, cudaStream_t st) {
+    static int per_sm = 0;
+    if (!per_sm) {
+        cudaError_t e =
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_march_kernel<MODEL, DIR>, 128, 0);
+        if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    }
+    const int warps = std::max(1, std::min(a.ntiles, per_sm * sms * 4));
+    MixedArgs b = a;
+    b.chunk = (a.ntiles + warps - 1) / warps;
+    const int busy = (a.ntiles + b.chunk - 1) / b.chunk;
+    mixed_march_kernel<MODEL, DIR><<<(busy + 3) / 4, 128, 0, st>>>(b);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "march launch: %s", cudaGetErrorString(e));
+    return CFD_OK;
+}
+
 template <int MODEL>
 int launch_shape(int dir, int shape, const MixedArgs& a, int grid, cudaStream_t st) {
     if (dir == DIR_X) {
@@ -89,6 +114,7 @@ int launch_shape(int dir, int shape, const MixedArgs& a, int grid, cudaStream_t 
     switch (shape) {
         case 0: return launch_t<MODEL, DIR_Y, 28, 8>(a, grid, st);
         case 1: return launch_t<MODEL, DIR_Y, 60, 4>(a, grid, st);
+        case kMarchShape: return launch_march<MODEL, DIR_Y>(a, grid, st);
         default: return launch_t<MODEL, DIR_Y, 12, 16>(a, grid, st);
     }
 }
@@ -288,7 +314,8 @@ struct cfd_batch {
     };
     std::vector<Group> groups;
     bool dirty = true;
-    int shape[2][2] = {{0, 0}, {0, 0}};  // [model][dir]
+    // [model][dir]; Euler y sweeps march by default (measured fastest on B200)
+    int shape[2][2] = {{0, kMarchShape}, {0, 0}};
     int sms = 148;
     // graph of `graph_steps` ticks for the current membership
     cudaGraphExec_t graph = nullptr;
@@ -446,9 +473,8 @@ size_t member_bytes(const cfd_config& c, size_t* plane_out, int* pitch_out) {
     int pitch = (c.nx + 31) / 32 * 32;
     size_t plane = (size_t)pitch * c.ny;
     int ty = 0;
-    for (int s = 0; s < kNumShapes; ++s)
-        ty = std::max(ty, std::max(tiles_for(c.nx, c.ny, DIR_Y, kShapesY[s]),
-                                   tiles_for(c.nx, c.ny, DIR_X, kShapesX[s])));
+    for (int s = 0; s < kNumShapesX; ++s) ty = std::max(ty, tiles_for(c.nx, c.ny, DIR_X, kShapesX[s]));
+    for (int s = 0; s < kNumShapesY; ++s) ty = std::max(ty, tiles_for(c.nx, c.ny, DIR_Y, kShapesY[s]));
     int npart = std::max(ty, kInitBlocks);
     size_t bytes = 4 * sizeof(float) * nv * plane  // value/compensation x 2 buffers
                    + 256 + sizeof(DevState) + 4 * sizeof(double) * npart + 4096;
@@ -765,8 +791,8 @@ int cfd_batch_size(cfd_batch* b, int* count, size_t* used, size_t* budget) {
 }
 
 int cfd_batch_set_shapes(cfd_batch* b, int model, int shape_x, int shape_y) {
-    if (!b || model < 0 || model > 1 || shape_x < 0 || shape_x >= kNumShapes || shape_y < 0 ||
-        shape_y >= kNumShapes)
+    if (!b || model < 0 || model > 1 || shape_x < 0 || shape_x >= kNumShapesX || shape_y < 0 ||
+        shape_y >= kNumShapesY)
         return cfd_fail(CFD_ERR_INVALID, "bad shape selection");
     b->shape[model][DIR_X] = shape_x;
     b->shape[model][DIR_Y] = shape_y;
@@ -797,7 +823,7 @@ int cfd_batch_autotune(cfd_batch* b, int steps_per_trial, double* best_ms) {
         for (int dir = 0; dir < 2; ++dir) {
             double best = 1e300;
             int best_s = b->shape[model][dir];
-            for (int s = 0; s < kNumShapes; ++s) {
+            for (int s = 0; s < (dir == DIR_X ? kNumShapesX : kNumShapesY); ++s) {
                 b->shape[model][dir] = s;
                 b->dirty = true;
                 int r = build_tables(b);

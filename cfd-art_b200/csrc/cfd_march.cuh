@@ -1,0 +1,333 @@
+// Mixed-precision sweeps by marching strips.
+//
+// A warp owns a strip of 32 lines x kMarchRows cells along the sweep of one
+// instance: lane = line, and every lane walks along its line one cell at a
+// time, keeping the last cells' primitive states, face states and flux in
+// registers.  The sweep therefore needs no shared memory and no barrier,
+// and re-reads only the two halo cells at each end of the strip.  In the y
+// sweep the lanes are 32 consecutive columns, so every step reads 32
+// consecutive cells (coalesced).  The code also has the x form (lanes on 32
+// rows, each lane reading consecutive cells of its row step by step), but
+// on B200 that form measured 1.9x slower than the tiled x sweep and its
+// contractions differ from the tiled ones, so the batch uses marching for y
+// only.  The arithmetic of every cell, face
+// and update is the one of the tiled sweep (cfd_mixed.cuh): the same
+// functions in the same order, so the two give the same results bit for bit
+// and the autotuner may pick either.
+//
+// Reduction: each strip reduces its lanes' wave speeds and masses into its
+// own slot of the instance's partials; the strip that completes the
+// instance's ticket count combines the slots in slot order (reproducible
+// sums) and picks the instance's dt.
+#pragma once
+
+#include "cfd_mixed.cuh"
+
+namespace cfd {
+namespace mixed {
+
+constexpr int kMarchRows = 64;  // rows of a strip (its width is one warp)
+
+// Raw (unrotated) cell of buffer `buf` at position `along` of line `line`.
+template <int MODEL, int DIR>
+__device__ __forceinline__ void march_load(const Inst& I, int buf, int along, int line, float* h,
+                                           float* l) {
+    const long long off = DIR == DIR_Y ? (long long)along * I.pitch + line
+                                       : (long long)line * I.pitch + along;
+    load_cell<MODEL>(I, buf, off, h, l);
+}
+
+// y-sweep frame: the boundary sign of a mirrored row, then (u, v) -> (v, -u).
+template <int MODEL>
+__device__ __forceinline__ void march_rotate_in(float* h, float* l, bool neg) {
+    using MT = ModelTraits<MODEL>;
+    if (neg) {
+        h[MT::IT] = -h[MT::IT];
+        l[MT::IT] = -l[MT::IT];
+    }
+    float t = h[MT::IM], tl = l[MT::IM];
+    h[MT::IM] = h[MT::IT];
+    l[MT::IM] = l[MT::IT];
+    h[MT::IT] = -t;
+    l[MT::IT] = -tl;
+}
+
+// Sweep frame of a loaded cell: the boundary sign of a mirrored cell (normal
+// momentum), and in y the rotation (u, v) -> (v, -u).
+template <int MODEL, int DIR>
+__device__ __forceinline__ void march_frame_in(float* h, float* l, bool neg) {
+    using MT = ModelTraits<MODEL>;
+    if (DIR == DIR_Y) {
+        march_rotate_in<MODEL>(h, l, neg);
+    } else if (neg) {
+        h[MT::IM] = -h[MT::IM];
+        l[MT::IM] = -l[MT::IM];
+    }
+}
+
+// Last-strip finish of the wave-speed reduction, by one warp: slots in slot
+// order per lane, then a fixed shuffle tree (reproducible sums).
+__device__ __forceinline__ void march_finish(DevState* st, const double* partials, int nslots,
+                                             double dt_used) {
+    const int lane = threadIdx.x & 31;
+    double mu = 0.0, mv = 0.0, m1 = 0.0, m2 = 0.0;
+    for (int b = lane; b < nslots; b += 32) {
+        mu = smax(mu, __ldcg(partials + 4 * b + 0));
+        mv = smax(mv, __ldcg(partials + 4 * b + 1));
+        m1 += __ldcg(partials + 4 * b + 2);
+        m2 += __ldcg(partials + 4 * b + 3);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mu = smax(mu, __shfl_down_sync(0xffffffffu, mu, o));
+        mv = smax(mv, __shfl_down_sync(0xffffffffu, mv, o));
+        m1 += __shfl_down_sync(0xffffffffu, m1, o);
+        m2 += __shfl_down_sync(0xffffffffu, m2, o);
+    }
+    if (lane == 0) {
+        DevState s = *st;
+        s.t = s.t + dt_used;
+        s.n = s.n + 1;
+        if (fabs(s.t - s.T) < 1e-12) s.t = s.T;
+        s.maxu = mu;
+        s.maxv = mv;
+        s.mass1 = m1 * s.dx * s.dy;
+        s.mass2 = m2 * s.dx * s.dy;
+        s.dt = choose_dt(s, mu, mv);
+        s.done = !(s.t < s.T);
+        s.ticket = 0;
+        *st = s;
+        __threadfence();
+    }
+}
+
+// One strip: cells [r0, r1) along the sweep of lines [b_org, b_org + 32) of
+// instance g.inst ("row" below means a position along the sweep).
+template <int MODEL, int DIR>
+__device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& g) {
+    using MT = ModelTraits<MODEL>;
+    constexpr int NV = MT::NV;
+    const int lane = threadIdx.x & 31;
+    const Inst& I = A.insts[g.inst];
+    const MPar P = load_par(I);
+    DevState* st = I.st;
+    const double dt = st->dt;
+    const double h_flux = DIR == DIR_X ? I.dx : (I.fix_dy ? I.dy : I.dx);
+    const float s_half = (float)(0.5 * (dt / h_flux));
+    const float k_upd = (float)(dt / (DIR == DIR_X ? I.dx : I.dy));
+    const int ny = g.len, nx = g.wid;  // cells along the sweep, lines
+    const int col = g.b_org + lane;    // this lane's line
+    const bool live = col < nx;
+    const int c = min(col, nx - 1);
+    const int r0 = g.a_org + 2;
+    const int r1 = min(r0 + kMarchRows, ny);
+    // the x sweep reads the current buffer, the y sweep the x sweep's output
+    const int bin = DIR == DIR_X ? g.cur : g.cur ^ 1, bout = bin ^ 1;
+    const int wall_bit = DIR == DIR_X ? 5 : 7;  // walls L, R / B, T
+    const bool wall_lo = (P.flags >> wall_bit) & 1, wall_hi = (P.flags >> (wall_bit + 1)) & 1;
+    const bool god = P.godunov();
+    const int lim = P.limiter();
+
+    // the mirrored source row of input row k and its sign
+    auto src_row = [&](int k, bool& neg) {
+        neg = false;
+        int r = k;
+        if (k < 0) {
+            r = -k - 1;
+            neg = wall_lo;
+        } else if (k >= ny) {
+            r = 2 * ny - 1 - k;
+            neg = wall_hi;
+        }
+        return min(max(r, 0), ny - 1);
+    };
+
+    float W1[NV], W2[NV];       // W(k-1), W(k-2)
+    float Pp[NV];               // state at the high face of row k-2
+    unsigned flp = 0;           // physicality flags of row k-2
+    float Flow[NV];             // flux at the low face of row k-2
+    float us_low = 0.f, zs_low = 0.f;
+    float z3 = 0.f;             // z of row k-3 (first-order z update)
+    float rmu = 0.f, rmv = 0.f;
+    double rm1 = 0.0, rm2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) W1[q] = W2[q] = Pp[q] = Flow[q] = 0.f;
+
+    // next row's raw cell, loaded one iteration ahead (in registers: on
+    // this kernel a shared-memory staging of the rows ahead measured slower)
+    float nh[NV], nl[NV];
+    bool nneg;
+    march_load<MODEL, DIR>(I, bin, src_row(r0 - 2, nneg), c, nh, nl);
+
+    for (int k = r0 - 2; k <= r1 + 1; ++k) {
+        float h[NV], l[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            h[q] = nh[q];
+            l[q] = nl[q];
+        }
+        const bool neg = nneg;
+        if (k + 1 <= r1 + 1) march_load<MODEL, DIR>(I, bin, src_row(k + 1, nneg), c, nh, nl);
+        march_frame_in<MODEL, DIR>(h, l, neg);
+        float W0[NV];
+        c2p_mixed<MODEL>(I, P, h, l, W0);
+
+        // slopes and evolved face states of row k-1
+        float Pn[NV], Mn[NV];
+        unsigned fln = 0;
+        if (k >= r0 && !god) {
+            float d[NV], X[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) d[q] = limit_f(lim, W1[q] - W2[q], W0[q] - W1[q]);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) Pn[q] = W1[q] + 0.5f * d[q];
+            if (phys_prim<MODEL>(P, Pn)) fln |= 1u;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) Pn[q] = W1[q] - 0.5f * d[q];
+            if (phys_prim<MODEL>(P, Pn)) fln |= 2u;
+            jac_f<MODEL>(P, W1, d, s_half, X);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) Pn[q] = (W1[q] + 0.5f * d[q]) - X[q];
+            if (phys_prim<MODEL>(P, Pn)) fln |= 4u;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) Mn[q] = (W1[q] - 0.5f * d[q]) - X[q];
+            if (phys_prim<MODEL>(P, Mn)) fln |= 8u;
+        }
+
+        // HLLC at the face between rows k-2 and k-1
+        float Fh[NV + 2];
+        if (k >= r0 + 1) {
+            float WL[NV], WR[NV];
+            const bool second = !god && (flp & 1u) && (fln & 2u) && (flp & 4u) && (fln & 8u);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                WL[q] = second ? Pp[q] : W2[q];
+                WR[q] = second ? Mn[q] : W1[q];
+            }
+            hllc_prim<MODEL>(P, WL, WR, Fh);
+        }
+
+        // compensated update of row k-2
+        if (k >= r0 + 2) {
+            const int row = k - 2;  // inside [r0, r1): no mirror, no sign
+            float hh[NV], ll[NV];
+            march_load<MODEL, DIR>(I, bin, row, c, hh, ll);
+            march_frame_in<MODEL, DIR>(hh, ll, false);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                if (MODEL == MODEL_ALLAIRE && q == 5) continue;
+                comp_add(hh[q], ll[q], k_upd * (Flow[q] - Fh[q]));
+            }
+            if constexpr (MODEL == MODEL_ALLAIRE) {
+                const float usL = us_low, usR = Fh[NV], zsL = zs_low, zsR = Fh[NV + 1];
+                const float z = hh[5];
+                float dz;
+                if (god)
+                    dz = -k_upd * ((W1[5] - z) * fminf_s(0.0f, usR) + (z - z3) * fmaxf_s(0.0f, usL));
+                else
+                    dz = -k_upd * ((usR * zsR - usL * zsL) - z * (usR - usL));
+                comp_add(hh[5], ll[5], dz);
+                float zlo = (float)I.z_min, zhi = (float)(1.0 - I.z_min);
+                if (hh[5] + ll[5] < zlo) { hh[5] = zlo; ll[5] = (float)(I.z_min - (double)zlo); }
+                if (hh[5] + ll[5] > zhi) { hh[5] = zhi; ll[5] = (float)((1.0 - I.z_min) - (double)zhi); }
+                if (hh[0] < 0.0f) { hh[0] = 0.0f; ll[0] = 0.0f; }
+                if (hh[1] < 0.0f) { hh[1] = 0.0f; ll[1] = 0.0f; }
+            }
+            if (DIR == DIR_Y) {  // rotate back
+                float t = hh[MT::IM], tl = ll[MT::IM];
+                hh[MT::IM] = -hh[MT::IT];
+                ll[MT::IM] = -ll[MT::IT];
+                hh[MT::IT] = t;
+                ll[MT::IT] = tl;
+            }
+            float Wn[NV];
+            c2p_mixed<MODEL>(I, P, hh, ll, Wn);
+            if constexpr (MODEL == MODEL_EULER) {
+                // density / energy restore as in the plain form (rare)
+                if (!(hh[0] > 1e-12f) || !(Wn[3] + P.gp1 > 0.0f)) {
+                    float oh[NV], ol[NV], Wo[NV];  // the cell before the update
+                    march_load<MODEL, DIR>(I, bin, row, c, oh, ol);
+                    c2p_mixed<MODEL>(I, P, oh, ol, Wo);  // stored (unrotated) frame
+                    float rho = hh[0] > 1e-12f ? hh[0] : oh[0];
+                    float u = Wn[1], v = Wn[2];
+                    float p = (Wn[3] + P.gp1 > 0.0f) ? Wn[3] : Wo[3];
+                    hh[0] = rho; ll[0] = 0.f;
+                    hh[1] = rho * u; ll[1] = 0.f;
+                    hh[2] = rho * v; ll[2] = 0.f;
+                    hh[3] = (p + P.gp1) * P.i1 + 0.5f * rho * (u * u + v * v); ll[3] = 0.f;
+                    Wn[0] = rho;
+                    Wn[3] = p;
+                }
+            }
+            if (live) {
+                store_cell<MODEL>(I, bout,
+                                  DIR == DIR_Y ? (long long)row * I.pitch + c
+                                               : (long long)c * I.pitch + row,
+                                  hh, ll);
+            }
+            if (DIR == DIR_Y && live) {
+                float cs = sound_f<MODEL>(P, Wn);
+                rmu = fmaxf_s(rmu, fabsf(Wn[MT::IM]) + cs);
+                rmv = fmaxf_s(rmv, fabsf(Wn[MT::IT]) + cs);
+                rm1 += (double)hh[0] + (double)ll[0];
+                if constexpr (MODEL == MODEL_ALLAIRE) rm2 += (double)hh[1] + (double)ll[1];
+            }
+        }
+
+        // shift the window
+        if constexpr (MODEL == MODEL_ALLAIRE) z3 = W2[5];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            W2[q] = W1[q];
+            W1[q] = W0[q];
+            Pp[q] = Pn[q];
+        }
+        flp = fln;
+        if (k >= r0 + 1) {
+#pragma unroll
+            for (int q = 0; q < NV; ++q) Flow[q] = Fh[q];
+            us_low = Fh[NV];
+            zs_low = MODEL == MODEL_ALLAIRE ? Fh[NV + 1] : 0.f;
+        }
+    }
+
+    if (DIR == DIR_X) return;  // the y sweep reduces
+    // this strip's wave speeds and masses into its slot, then the ticket
+    double mu = (double)rmu, mv = (double)rmv;
+    for (int o = 16; o > 0; o >>= 1) {
+        mu = smax(mu, __shfl_down_sync(0xffffffffu, mu, o));
+        mv = smax(mv, __shfl_down_sync(0xffffffffu, mv, o));
+        rm1 += __shfl_down_sync(0xffffffffu, rm1, o);
+        rm2 += __shfl_down_sync(0xffffffffu, rm2, o);
+    }
+    unsigned ticket = 0;
+    if (lane == 0) {
+        double* p = I.partials + 4 * g.ltile;
+        p[0] = mu;
+        p[1] = mv;
+        p[2] = rm1;
+        p[3] = rm2;
+        __threadfence();
+        ticket = atomicAdd(&st->ticket, 1u);
+    }
+    ticket = __shfl_sync(0xffffffffu, ticket, 0);
+    if (ticket + 1u == (unsigned)I.tiles_y) {
+        __threadfence();
+        march_finish(st, I.partials, I.tiles_y, dt);
+    }
+}
+
+// Persistent sweep: warp w of the grid walks the strips
+// [w * chunk, (w + 1) * chunk) of the launch's strip list.
+template <int MODEL, int DIR>
+__global__ void __launch_bounds__(128) mixed_march_kernel(MixedArgs A) {
+    const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int t_begin = gw * A.chunk;
+    const int t_end = min(t_begin + A.chunk, A.ntiles);
+    for (int tile = t_begin; tile < t_end; ++tile) {
+        const TileGeom g = tile_geom<DIR, kMarchRows, 32>(A, tile);
+        if (!g.skip) march_strip<MODEL, DIR>(A, g);
+    }
+}
+
+}  // namespace mixed
+}  // namespace cfd

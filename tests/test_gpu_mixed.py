@@ -116,17 +116,20 @@ def test_member_alone_equals_member_in_mix():
 
 
 def test_tile_shapes_do_not_change_results():
+    """Three tiled shapes per direction and the marching y sweep (y shape 3)
+    give the same bits."""
     mem = _members()[:3]
     outs = []
-    for shape in range(3):
+    for shape in range(4):
         with G.Batch() as b:
             for model in (G.EULER, G.ALLAIRE):
-                b.set_shapes(model, shape, shape)
+                b.set_shapes(model, min(shape, 2), shape)
             ids = [b.add(c, ic, 20) for c, ic, _ in mem]
             b.step(20)
             outs.append([b.download(i) for i in ids])
     for k in range(len(mem)):
-        assert np.array_equal(outs[0][k], outs[1][k]) and np.array_equal(outs[0][k], outs[2][k])
+        for o in outs[1:]:
+            assert np.array_equal(outs[0][k], o[k])
 
 
 def test_autotune_keeps_results_and_picks_shapes():
