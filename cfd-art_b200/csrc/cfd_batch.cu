@@ -3,7 +3,8 @@
 // A batch owns device state for each member solve (instance) and advances
 // all active instances by one split step per "tick": one persistent x-sweep
 // launch and one persistent y-sweep launch per model present, over a tile
-// list that covers every active instance (csrc/cfd_mixed.cuh).  Each instance
+// list that covers every active instance (x: warp segments, csrc/cfd_march.cuh;
+// y: shared-memory tiles, csrc/cfd_mixed.cuh, or marching strips).  Each instance
 // keeps its own time-loop state (n, t, dt, T, max_steps), picks its own dt
 // after each step and stops on its own.  Ticks are captured into a CUDA graph
 // that is replayed until the membership changes.  Instances are admitted
@@ -50,12 +51,14 @@ namespace {
 struct Shape {
     int ts, na;
 };
-// y shape 3: marching strips of 32 columns x kMarchRows rows (cfd_march.cuh);
-// in x the marching form (lanes on 32 different rows) measured 1.9x slower
-// than the tiles, so x keeps the three tile shapes
-constexpr Shape kShapesX[] = {{60, 4}, {124, 2}, {28, 8}};
+// x: warp segments of kSegCells columns x kSegRows rows (cfd_march.cuh), the
+// only x form (it measured 13-25 % faster than every tile shape, and a single
+// x form keeps results independent of the autotuner's choice).
+// y: three tile shapes, and shape 3 = marching strips of 32 columns x
+// kMarchRows rows (cfd_march.cuh), bit-identical to the tiles.
+constexpr Shape kShapesX[] = {{kSegCells, kSegRows}};
 constexpr Shape kShapesY[] = {{28, 8}, {60, 4}, {12, 16}, {kMarchRows, 32}};
-constexpr int kNumShapesX = 3, kNumShapesY = 4;
+constexpr int kNumShapesX = 1, kNumShapesY = 4;
 constexpr int kMarchShape = 3;
 
 // Persistent launch: as many CTAs as fit on the device at once (occupancy
@@ -102,15 +105,28 @@ int launch_march(const MixedArgs& a, int sms, cudaStream_t st) {
     return CFD_OK;
 }
 
+// Persistent warp-segment x sweep (4-warp CTAs), launched like the marching one.
+template <int MODEL>
+int launch_segment(const MixedArgs& a, int sms, cudaStream_t st) {
+    static int per_sm = 0;
+    if (!per_sm) {
+        cudaError_t e =
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_segment_x_kernel<MODEL>, 128, 0);
+        if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    }
+    const int warps = std::max(1, std::min(a.ntiles, per_sm * sms * 4));
+    MixedArgs b = a;
+    b.chunk = (a.ntiles + warps - 1) / warps;
+    const int busy = (a.ntiles + b.chunk - 1) / b.chunk;
+    mixed_segment_x_kernel<MODEL><<<(busy + 3) / 4, 128, 0, st>>>(b);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "segment launch: %s", cudaGetErrorString(e));
+    return CFD_OK;
+}
+
 template <int MODEL>
 int launch_shape(int dir, int shape, const MixedArgs& a, int grid, cudaStream_t st) {
-    if (dir == DIR_X) {
-        switch (shape) {
-            case 0: return launch_t<MODEL, DIR_X, 60, 4>(a, grid, st);
-            case 1: return launch_t<MODEL, DIR_X, 124, 2>(a, grid, st);
-            default: return launch_t<MODEL, DIR_X, 28, 8>(a, grid, st);
-        }
-    }
+    if (dir == DIR_X) return launch_segment<MODEL>(a, grid, st);
     switch (shape) {
         case 0: return launch_t<MODEL, DIR_Y, 28, 8>(a, grid, st);
         case 1: return launch_t<MODEL, DIR_Y, 60, 4>(a, grid, st);
@@ -823,7 +839,8 @@ int cfd_batch_autotune(cfd_batch* b, int steps_per_trial, double* best_ms) {
         for (int dir = 0; dir < 2; ++dir) {
             double best = 1e300;
             int best_s = b->shape[model][dir];
-            for (int s = 0; s < (dir == DIR_X ? kNumShapesX : kNumShapesY); ++s) {
+            const int nshapes = dir == DIR_X ? kNumShapesX : kNumShapesY;
+            for (int s = 0; s < nshapes; ++s) {
                 b->shape[model][dir] = s;
                 b->dirty = true;
                 int r = build_tables(b);

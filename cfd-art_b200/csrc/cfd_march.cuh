@@ -329,5 +329,172 @@ __global__ void __launch_bounds__(128) mixed_march_kernel(MixedArgs A) {
     }
 }
 
+// ---- x sweep by warp segments ------------------------------------------------
+// A warp owns a tile of kSegCells columns x kSegRows rows and walks its rows:
+// the 32 lanes hold 32 consecutive cells of a row (kSegCells outputs plus a
+// 2-cell halo at each end), so every load and store is coalesced, and the
+// neighbours each stencil step needs (primitive states, face states, fluxes)
+// come from the adjacent lanes by warp shuffles: no shared memory, no
+// barrier.  The arithmetic is the tiled sweep's, in the same order.
+constexpr int kSegCells = 28;  // outputs per row segment
+constexpr int kSegRows = 16;   // rows of a tile
+
+template <int N>
+__device__ __forceinline__ void shfl_up_n(const float* x, float* y) {
+#pragma unroll
+    for (int q = 0; q < N; ++q) y[q] = __shfl_up_sync(0xffffffffu, x[q], 1);
+}
+template <int N>
+__device__ __forceinline__ void shfl_down_n(const float* x, float* y) {
+#pragma unroll
+    for (int q = 0; q < N; ++q) y[q] = __shfl_down_sync(0xffffffffu, x[q], 1);
+}
+
+template <int MODEL>
+__device__ __forceinline__ void segment_tile(const MixedArgs& A, const TileGeom& g) {
+    using MT = ModelTraits<MODEL>;
+    constexpr int NV = MT::NV;
+    const int lane = threadIdx.x & 31;
+    const Inst& I = A.insts[g.inst];
+    const MPar P = load_par(I);
+    const double dt = I.st->dt;
+    const float s_half = (float)(0.5 * (dt / I.dx));
+    const float k_upd = (float)(dt / I.dx);
+    const int nx = g.len, ny = g.wid;
+    const int bin = g.cur, bout = g.cur ^ 1;
+    const bool god = P.godunov();
+    const int lim = P.limiter();
+    // this lane's column and its mirrored source (pre_sweep's fill)
+    const int ga = g.a_org + lane;
+    int src = ga;
+    bool neg = false;
+    if (ga < 0) {
+        src = -ga - 1;
+        neg = (P.flags >> 5) & 1;
+    } else if (ga >= nx) {
+        src = 2 * nx - 1 - ga;
+        neg = (P.flags >> 6) & 1;
+    }
+    src = min(max(src, 0), nx - 1);
+    const bool writer = lane >= 2 && lane < 2 + kSegCells && ga < nx;
+    const int row_end = min(g.b_org + kSegRows, ny);
+
+    float nh[NV], nl[NV];
+    load_cell<MODEL>(I, bin, (long long)g.b_org * I.pitch + src, nh, nl);
+    for (int row = g.b_org; row < row_end; ++row) {
+        float h[NV], l[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            h[q] = nh[q];
+            l[q] = nl[q];
+        }
+        if (row + 1 < row_end) load_cell<MODEL>(I, bin, (long long)(row + 1) * I.pitch + src, nh, nl);
+        if (neg) {
+            h[MT::IM] = -h[MT::IM];
+            l[MT::IM] = -l[MT::IM];
+        }
+        float W[NV], Wl[NV], Wr[NV];
+        c2p_mixed<MODEL>(I, P, h, l, W);
+        shfl_up_n<NV>(W, Wl);
+        shfl_down_n<NV>(W, Wr);
+
+        // slopes and evolved face states of this cell (used by lanes 1..30)
+        float Pf[NV], Mf[NV];
+        unsigned fl = 0;
+        if (!god) {
+            float d[NV], X[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) d[q] = limit_f(lim, W[q] - Wl[q], Wr[q] - W[q]);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) Pf[q] = W[q] + 0.5f * d[q];
+            if (phys_prim<MODEL>(P, Pf)) fl |= 1u;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) Pf[q] = W[q] - 0.5f * d[q];
+            if (phys_prim<MODEL>(P, Pf)) fl |= 2u;
+            jac_f<MODEL>(P, W, d, s_half, X);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) Pf[q] = (W[q] + 0.5f * d[q]) - X[q];
+            if (phys_prim<MODEL>(P, Pf)) fl |= 4u;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) Mf[q] = (W[q] - 0.5f * d[q]) - X[q];
+            if (phys_prim<MODEL>(P, Mf)) fl |= 8u;
+        } else {
+#pragma unroll
+            for (int q = 0; q < NV; ++q) Pf[q] = Mf[q] = W[q];
+        }
+
+        // HLLC at this cell's low face (between the lane below and this one)
+        float PL[NV];
+        shfl_up_n<NV>(Pf, PL);
+        const unsigned flL = __shfl_up_sync(0xffffffffu, fl, 1);
+        float F[NV + 2];
+        {
+            float WL[NV], WR[NV];
+            const bool second = !god && (flL & 1u) && (fl & 2u) && (flL & 4u) && (fl & 8u);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                WL[q] = second ? PL[q] : Wl[q];
+                WR[q] = second ? Mf[q] : W[q];
+            }
+            hllc_prim<MODEL>(P, WL, WR, F);
+        }
+        float FR[NV + 2];
+        shfl_down_n<NV + 2>(F, FR);
+
+        // compensated update (lanes 2 .. 2 + kSegCells - 1)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            if (MODEL == MODEL_ALLAIRE && q == 5) continue;
+            comp_add(h[q], l[q], k_upd * (F[q] - FR[q]));
+        }
+        if constexpr (MODEL == MODEL_ALLAIRE) {
+            const float usL = F[NV], usR = FR[NV], zsL = F[NV + 1], zsR = FR[NV + 1];
+            const float z = h[5];
+            float dz;
+            if (god)
+                dz = -k_upd * ((Wr[5] - z) * fminf_s(0.0f, usR) + (z - Wl[5]) * fmaxf_s(0.0f, usL));
+            else
+                dz = -k_upd * ((usR * zsR - usL * zsL) - z * (usR - usL));
+            comp_add(h[5], l[5], dz);
+            float zlo = (float)I.z_min, zhi = (float)(1.0 - I.z_min);
+            if (h[5] + l[5] < zlo) { h[5] = zlo; l[5] = (float)(I.z_min - (double)zlo); }
+            if (h[5] + l[5] > zhi) { h[5] = zhi; l[5] = (float)((1.0 - I.z_min) - (double)zhi); }
+            if (h[0] < 0.0f) { h[0] = 0.0f; l[0] = 0.0f; }
+            if (h[1] < 0.0f) { h[1] = 0.0f; l[1] = 0.0f; }
+        }
+        if constexpr (MODEL == MODEL_EULER) {
+            float Wn[NV];
+            c2p_mixed<MODEL>(I, P, h, l, Wn);
+            // density / energy restore as in the plain form (rare)
+            if (writer && (!(h[0] > 1e-12f) || !(Wn[3] + P.gp1 > 0.0f))) {
+                float oh[NV], ol[NV], Wo[NV];  // the cell before the update
+                load_cell<MODEL>(I, bin, (long long)row * I.pitch + src, oh, ol);
+                c2p_mixed<MODEL>(I, P, oh, ol, Wo);
+                float rho = h[0] > 1e-12f ? h[0] : oh[0];
+                float u = Wn[1], v = Wn[2];
+                float p = (Wn[3] + P.gp1 > 0.0f) ? Wn[3] : Wo[3];
+                h[0] = rho; l[0] = 0.f;
+                h[1] = rho * u; l[1] = 0.f;
+                h[2] = rho * v; l[2] = 0.f;
+                h[3] = (p + P.gp1) * P.i1 + 0.5f * rho * (u * u + v * v); l[3] = 0.f;
+            }
+        }
+        if (writer) store_cell<MODEL>(I, bout, (long long)row * I.pitch + ga, h, l);
+    }
+}
+
+// Persistent x sweep: warp w of the grid walks the tiles
+// [w * chunk, (w + 1) * chunk) of the launch's tile list.
+template <int MODEL>
+__global__ void __launch_bounds__(128) mixed_segment_x_kernel(MixedArgs A) {
+    const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int t_begin = gw * A.chunk;
+    const int t_end = min(t_begin + A.chunk, A.ntiles);
+    for (int tile = t_begin; tile < t_end; ++tile) {
+        const TileGeom g = tile_geom<DIR_X, kSegCells, kSegRows>(A, tile);
+        if (!g.skip) segment_tile<MODEL>(A, g);
+    }
+}
+
 }  // namespace mixed
 }  // namespace cfd

@@ -17,6 +17,9 @@
 // table maps blockIdx to (instance, tile); each instance has its own grid,
 // materials, options, buffers and device-resident time state, and its y
 // sweep finishes its own wave-speed reduction (last CTA of that instance).
+// The batch runs this tiled form for the y sweep (with the marching strips
+// of cfd_march.cuh as an alternative); the x sweep uses the warp segments of
+// cfd_march.cuh.  The tiled code is written for both directions.
 #pragma once
 
 #include "cfd_physics.cuh"
