@@ -383,14 +383,14 @@ def bench_single(args, ctx, G, stream, clocks):
         launches = kn[0] + kn[1]
         dom = 0 if kms[0] >= kms[1] else 1
         rl = roofline(["sweep_x", "sweep_y"][dom], kms[dom], kn[dom], cells * nv * 8 * 2,
-                      f"{model}_sweep_{'xy'[dom]}")
+                      f"{model}_sweep_{'xy'[dom]}_{nx}")
     else:
         mx, my, n = s.step_timed(4)
         st = s.status(mid)
         launches = 2 * K
         dom = 0 if mx >= my else 1
         rl = roofline(["mixed_sweep_x", "mixed_sweep_y"][dom], [mx, my][dom], 4,
-                      cells * nv * 8 * 2, f"{model}_mixed_sweep_{'xy'[dom]}")
+                      cells * nv * 8 * 2, f"{model}_mixed_sweep_{'xy'[dom]}_{nx}")
     s.close()
     e2e = None
     if not args.no_e2e:
