@@ -22,6 +22,7 @@
 #include <map>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/cfdgpu.h"
@@ -54,10 +55,11 @@ struct Shape {
 // x: warp segments of kSegCells columns x kSegRows rows (cfd_march.cuh), the
 // only x form (it measured 13-25 % faster than every tile shape, and a single
 // x form keeps results independent of the autotuner's choice).
-// y: three tile shapes, and shape 3 = marching strips of 32 columns x
-// kMarchRows rows (cfd_march.cuh), bit-identical to the tiles.
+// y: three tile shapes, and shape 3 = marching strips of 32 columns
+// (cfd_march.cuh), bit-identical to the tiles; their length is chosen per
+// launch (march_rows), kMarchMaxRows is the nominal one.
 constexpr Shape kShapesX[] = {{kSegCells, kSegRows}};
-constexpr Shape kShapesY[] = {{28, 8}, {60, 4}, {12, 16}, {kMarchRows, 32}};
+constexpr Shape kShapesY[] = {{28, 8}, {60, 4}, {12, 16}, {kMarchMaxRows, 32}};
 constexpr int kNumShapesX = 1, kNumShapesY = 4;
 constexpr int kMarchShape = 3;
 
@@ -85,17 +87,23 @@ int launch_t(const MixedArgs& a, int sms, cudaStream_t st) {
     return CFD_OK;
 }
 
-// Persistent marching y sweep (4-warp CTAs): as many warps as fit on the device, each
-// walking a contiguous range of strips.
+// Resident 4-warp CTAs per SM of the marching sweep.
 template <int MODEL, int DIR>
-int launch_march(const MixedArgs& a, int sms, cudaStream_t st) {
+int march_per_sm() {
     static int per_sm = 0;
     if (!per_sm) {
         cudaError_t e =
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_march_kernel<MODEL, DIR>, 128, 0);
         if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     }
-    const int warps = std::max(1, std::min(a.ntiles, per_sm * sms * 4));
+    return per_sm;
+}
+
+// Persistent marching y sweep (4-warp CTAs): as many warps as fit on the device, each
+// walking a contiguous range of strips.
+template <int MODEL, int DIR>
+int launch_march(const MixedArgs& a, int sms, cudaStream_t st) {
+    const int warps = std::max(1, std::min(a.ntiles, march_per_sm<MODEL, DIR>() * sms * 4));
     MixedArgs b = a;
     b.chunk = (a.ntiles + warps - 1) / warps;
     const int busy = (a.ntiles + b.chunk - 1) / b.chunk;
@@ -138,6 +146,27 @@ int launch_shape(int dir, int shape, const MixedArgs& a, int grid, cudaStream_t 
 int tiles_for(int nx, int ny, int dir, Shape s) {
     int len = dir == DIR_X ? nx : ny, wid = dir == DIR_X ? ny : nx;
     return ((len + s.ts - 1) / s.ts) * ((wid + s.na - 1) / s.na);
+}
+
+// Strip length of a marching launch over strips of 32 columns of the given
+// grids: a warp walks ceil(strips / slots) strips one after the other, each
+// costing its length plus the 4 halo rows, so the length with the fewest
+// (rounds x (rows + 4)) is taken, the longest on ties.  Grids with few
+// strips get shorter ones, so that they still fill the resident warps.
+int march_rows(const std::vector<std::pair<int, int>>& grids, long long slots) {
+    int best = kMarchMaxRows;
+    long long best_cost = -1;
+    for (int rows = kMarchMaxRows; rows >= kMarchMinRows; rows -= 4) {
+        long long strips = 0;
+        for (const auto& g : grids) strips += (long long)((g.first + 31) / 32) * ((g.second + rows - 1) / rows);
+        if (!strips) return kMarchMaxRows;
+        const long long cost = (strips + slots - 1) / slots * (rows + 4);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = rows;
+        }
+    }
+    return best;
 }
 
 // ---- conversion kernels ----------------------------------------------------
@@ -327,6 +356,7 @@ struct cfd_batch {
     size_t d_tiles_cap = 0;
     struct Group {
         int model, dir, shape, ntiles, offset;
+        int rows;  // marching strips: cells along the sweep per strip
     };
     std::vector<Group> groups;
     bool dirty = true;
@@ -374,12 +404,24 @@ int build_tables(cfd_batch* b) {
     if (int r = wait_uploads(b)) return r;
     if (!b->dirty) return CFD_OK;
     b->groups.clear();
+    // the y shape of each model, with the strip length of a marching sweep
+    Shape shape_y[2];
+    for (int model = 0; model < 2; ++model) {
+        shape_y[model] = kShapesY[b->shape[model][DIR_Y]];
+        if (b->shape[model][DIR_Y] != kMarchShape) continue;
+        std::vector<std::pair<int, int>> grids;
+        for (const Member& m : b->members)
+            if (m.cfg.model == model && !m.final) grids.emplace_back(m.cfg.nx, m.cfg.ny);
+        const int per_sm = model == CFD_MODEL_EULER ? march_per_sm<MODEL_EULER, DIR_Y>()
+                                                    : march_per_sm<MODEL_ALLAIRE, DIR_Y>();
+        shape_y[model].ts = march_rows(grids, (long long)per_sm * b->sms * 4);
+    }
     std::vector<Inst> insts(b->members.size());
     for (size_t i = 0; i < b->members.size(); ++i) {
         Member& m = b->members[i];
         int model = m.cfg.model;
         m.inst.tiles_x = tiles_for(m.cfg.nx, m.cfg.ny, DIR_X, kShapesX[b->shape[model][DIR_X]]);
-        m.inst.tiles_y = tiles_for(m.cfg.nx, m.cfg.ny, DIR_Y, kShapesY[b->shape[model][DIR_Y]]);
+        m.inst.tiles_y = tiles_for(m.cfg.nx, m.cfg.ny, DIR_Y, shape_y[model]);
         insts[i] = m.inst;
     }
     // largest instances first within each group so the tail of a sweep is
@@ -398,7 +440,8 @@ int build_tables(cfd_batch* b) {
             g.dir = dir;
             g.shape = b->shape[model][dir];
             g.offset = (int)all.size();
-            const Shape sh = dir == DIR_X ? kShapesX[g.shape] : kShapesY[g.shape];
+            const Shape sh = dir == DIR_X ? kShapesX[g.shape] : shape_y[model];
+            g.rows = sh.ts;
             for (int idx : order) {
                 const Member& m = b->members[idx];
                 if (m.cfg.model != model || m.final) continue;  // finished: no tiles
@@ -465,6 +508,7 @@ int enqueue_tick(cfd_batch* b, std::vector<Timed>* timing) {
             a.insts = b->d_insts;
             a.tiles = b->d_tiles + g.offset;
             a.ntiles = g.ntiles;
+            a.rows = g.rows;
             cudaEvent_t e0 = nullptr, e1 = nullptr;
             if (timing) {
                 cudaEventCreate(&e0);
@@ -491,6 +535,7 @@ size_t member_bytes(const cfd_config& c, size_t* plane_out, int* pitch_out) {
     int ty = 0;
     for (int s = 0; s < kNumShapesX; ++s) ty = std::max(ty, tiles_for(c.nx, c.ny, DIR_X, kShapesX[s]));
     for (int s = 0; s < kNumShapesY; ++s) ty = std::max(ty, tiles_for(c.nx, c.ny, DIR_Y, kShapesY[s]));
+    ty = std::max(ty, tiles_for(c.nx, c.ny, DIR_Y, Shape{kMarchMinRows, 32}));  // shortest strips
     int npart = std::max(ty, kInitBlocks);
     size_t bytes = 4 * sizeof(float) * nv * plane  // value/compensation x 2 buffers
                    + 256 + sizeof(DevState) + 4 * sizeof(double) * npart + 4096;

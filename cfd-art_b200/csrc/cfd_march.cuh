@@ -1,9 +1,10 @@
 // Mixed-precision sweeps by marching strips.
 //
-// A warp owns a strip of 32 lines x kMarchRows cells along the sweep of one
+// A warp owns a strip of 32 lines x A.rows cells along the sweep of one
 // instance: lane = line, and every lane walks along its line one cell at a
-// time, keeping the last cells' primitive states, face states and flux in
-// registers.  The sweep therefore needs no shared memory and no barrier,
+// time, keeping the last cells' primitive states, face states, raw cells and
+// flux in registers.  The strip length is chosen per launch on the host
+// (kMarchMinRows..kMarchMaxRows) so that the strips fill the resident warps.  The sweep therefore needs no shared memory and no barrier,
 // and re-reads only the two halo cells at each end of the strip.  In the y
 // sweep the lanes are 32 consecutive columns, so every step reads 32
 // consecutive cells (coalesced).  The code also has the x form (lanes on 32
@@ -26,7 +27,7 @@
 namespace cfd {
 namespace mixed {
 
-constexpr int kMarchRows = 64;  // rows of a strip (its width is one warp)
+constexpr int kMarchMaxRows = 64, kMarchMinRows = 16;  // rows of a strip (its width is one warp)
 
 // Raw (unrotated) cell of buffer `buf` at position `along` of line `line`.
 template <int MODEL, int DIR>
@@ -119,7 +120,7 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
     const bool live = col < nx;
     const int c = min(col, nx - 1);
     const int r0 = g.a_org + 2;
-    const int r1 = min(r0 + kMarchRows, ny);
+    const int r1 = min(r0 + A.rows, ny);
     // the x sweep reads the current buffer, the y sweep the x sweep's output
     const int bin = DIR == DIR_X ? g.cur : g.cur ^ 1, bout = bin ^ 1;
     const int wall_bit = DIR == DIR_X ? 5 : 7;  // walls L, R / B, T
@@ -152,6 +153,11 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
 #pragma unroll
     for (int q = 0; q < NV; ++q) W1[q] = W2[q] = Pp[q] = Flow[q] = 0.f;
 
+    // raw cells of rows k-1 and k-2 in the sweep frame (the update of row
+    // k-2 starts from them; a reload from global memory measured 5 % slower)
+    float H1[NV], L1[NV], H2[NV], L2[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) H1[q] = L1[q] = H2[q] = L2[q] = 0.f;
     // next row's raw cell, loaded one iteration ahead (in registers: on
     // this kernel a shared-memory staging of the rows ahead measured slower)
     float nh[NV], nl[NV];
@@ -210,8 +216,11 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
         if (k >= r0 + 2) {
             const int row = k - 2;  // inside [r0, r1): no mirror, no sign
             float hh[NV], ll[NV];
-            march_load<MODEL, DIR>(I, bin, row, c, hh, ll);
-            march_frame_in<MODEL, DIR>(hh, ll, false);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                hh[q] = H2[q];  // row k-2 as loaded, in the sweep frame
+                ll[q] = L2[q];
+            }
 #pragma unroll
             for (int q = 0; q < NV; ++q) {
                 if (MODEL == MODEL_ALLAIRE && q == 5) continue;
@@ -277,6 +286,10 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
         if constexpr (MODEL == MODEL_ALLAIRE) z3 = W2[5];
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
+            H2[q] = H1[q];
+            L2[q] = L1[q];
+            H1[q] = h[q];
+            L1[q] = l[q];
             W2[q] = W1[q];
             W1[q] = W0[q];
             Pp[q] = Pn[q];
@@ -324,7 +337,7 @@ __global__ void __launch_bounds__(128) mixed_march_kernel(MixedArgs A) {
     const int t_begin = gw * A.chunk;
     const int t_end = min(t_begin + A.chunk, A.ntiles);
     for (int tile = t_begin; tile < t_end; ++tile) {
-        const TileGeom g = tile_geom<DIR, kMarchRows, 32>(A, tile);
+        const TileGeom g = tile_geom<DIR, kMarchMaxRows, 32>(A, tile);
         if (!g.skip) march_strip<MODEL, DIR>(A, g);
     }
 }

@@ -73,6 +73,7 @@ struct MixedArgs {
     const TileEnt* tiles;   // tiles of this launch
     int ntiles;             // tiles of this launch
     int chunk;              // CTA c walks tiles [c * chunk, (c + 1) * chunk) (persistent)
+    int rows;               // marching strips: cells along the sweep per strip
 };
 
 // Per-tile constants held in registers (one vector load per tile instead of
