@@ -182,8 +182,7 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
         unsigned fln = 0;
         if (k >= r0 && !god) {
             float d[NV], X[NV];
-#pragma unroll
-            for (int q = 0; q < NV; ++q) d[q] = limit_f(lim, W1[q] - W2[q], W0[q] - W1[q]);
+            limit_all<NV>(lim, W2, W1, W0, d);
 #pragma unroll
             for (int q = 0; q < NV; ++q) Pn[q] = W1[q] + 0.5f * d[q];
             if (phys_prim<MODEL>(P, Pn)) fln |= 1u;
@@ -416,8 +415,7 @@ __device__ __forceinline__ void segment_tile(const MixedArgs& A, const TileGeom&
         unsigned fl = 0;
         if (!god) {
             float d[NV], X[NV];
-#pragma unroll
-            for (int q = 0; q < NV; ++q) d[q] = limit_f(lim, W[q] - Wl[q], Wr[q] - W[q]);
+            limit_all<NV>(lim, Wl, W, Wr, d);
 #pragma unroll
             for (int q = 0; q < NV; ++q) Pf[q] = W[q] + 0.5f * d[q];
             if (phys_prim<MODEL>(P, Pf)) fl |= 1u;

@@ -211,6 +211,30 @@ __device__ __forceinline__ float limit_f(int lim, float a, float b) {
     }
 }
 
+// Limited slopes of all components, d = limit(W - Wm, Wp - W), with the
+// limiter chosen once for the cell rather than once per component.
+template <int NV>
+__device__ __forceinline__ void limit_all(int lim, const float* Wm, const float* W, const float* Wp,
+                                          float* d) {
+    switch (lim) {
+        case LIM_VANLEER:
+#pragma unroll
+            for (int q = 0; q < NV; ++q) d[q] = limit_f(LIM_VANLEER, W[q] - Wm[q], Wp[q] - W[q]);
+            break;
+        case LIM_MC:
+#pragma unroll
+            for (int q = 0; q < NV; ++q) d[q] = limit_f(LIM_MC, W[q] - Wm[q], Wp[q] - W[q]);
+            break;
+        case LIM_UNLIMITED:
+#pragma unroll
+            for (int q = 0; q < NV; ++q) d[q] = limit_f(LIM_UNLIMITED, W[q] - Wm[q], Wp[q] - W[q]);
+            break;
+        default:
+#pragma unroll
+            for (int q = 0; q < NV; ++q) d[q] = limit_f(LIM_MINMOD, W[q] - Wm[q], Wp[q] - W[q]);
+    }
+}
+
 // Sound speed of a primitive state.
 template <int MODEL> __device__ __forceinline__ float sound_f(const MPar& P, const float* W) {
     if constexpr (MODEL == MODEL_EULER) {
@@ -572,8 +596,7 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
         sW.get(s, W);
         sW.get(s - ST, Wl);
         sW.get(s + ST, Wr);
-#pragma unroll
-        for (int k = 0; k < NV; ++k) d[k] = limit_f(P.limiter(), W[k] - Wl[k], Wr[k] - W[k]);
+        limit_all<NV>(P.limiter(), Wl, W, Wr, d);
         unsigned fl = 0;
 #pragma unroll
         for (int k = 0; k < NV; ++k) Wt[k] = W[k] + 0.5f * d[k];

@@ -235,6 +235,31 @@ __device__ __forceinline__ double limit1(int lim, double a, double b) {
     }
 }
 
+// Limited slopes of all components, d = limit(W - Wm, Wp - W), with the
+// limiter chosen once for the cell rather than once per component (the
+// arithmetic of each component is limit1's).
+template <int NV>
+__device__ __forceinline__ void limit_all1(int lim, const double* Wm, const double* W,
+                                           const double* Wp, double* d) {
+    switch (lim) {
+        case LIM_VANLEER:
+#pragma unroll
+            for (int k = 0; k < NV; ++k) d[k] = limit1(LIM_VANLEER, W[k] - Wm[k], Wp[k] - W[k]);
+            break;
+        case LIM_MC:
+#pragma unroll
+            for (int k = 0; k < NV; ++k) d[k] = limit1(LIM_MC, W[k] - Wm[k], Wp[k] - W[k]);
+            break;
+        case LIM_UNLIMITED:
+#pragma unroll
+            for (int k = 0; k < NV; ++k) d[k] = limit1(LIM_UNLIMITED, W[k] - Wm[k], Wp[k] - W[k]);
+            break;
+        default:
+#pragma unroll
+            for (int k = 0; k < NV; ++k) d[k] = limit1(LIM_MINMOD, W[k] - Wm[k], Wp[k] - W[k]);
+    }
+}
+
 // ------------------------------------------------ MUSCL-Hancock half step ---
 // E/headers/flux_solver_MUSCLhancock.hpp:195-201 with the Jacobian of
 // E/headers/misc_euler.hpp:102-119 (A/headers/misc.hpp:189-205 for Allaire):

@@ -301,8 +301,7 @@ __global__ void __launch_bounds__(256, MODEL == MODEL_EULER ? 3 : 2) sweep_kerne
                 Wl[k] = sWF[k * NSLOT + s - ST];
                 Wr[k] = sWF[k * NSLOT + s + ST];
             }
-#pragma unroll
-            for (int k = 0; k < NV; ++k) d[k] = limit1(A.limiter, P.W[k] - Wl[k], Wr[k] - P.W[k]);
+            limit_all1<NV>(A.limiter, Wl, P.W, Wr, d);
             if constexpr (MODEL == MODEL_EULER) {
                 P.rho = P.W[0];
             } else {
