@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(128) mixed_march_kernel(MixedArgs A) {
 // come from the adjacent lanes by warp shuffles: no shared memory, no
 // barrier.  The arithmetic is the tiled sweep's, in the same order.
 constexpr int kSegCells = 28;  // outputs per row segment
-constexpr int kSegRows = 16;   // rows of a tile
+constexpr int kSegRows = 32;   // rows of a tile
 
 template <int N>
 __device__ __forceinline__ void shfl_up_n(const float* x, float* y) {
@@ -495,9 +495,12 @@ __device__ __forceinline__ void segment_tile(const MixedArgs& A, const TileGeom&
 }
 
 // Persistent x sweep: warp w of the grid walks the tiles
-// [w * chunk, (w + 1) * chunk) of the launch's tile list.
+// [w * chunk, (w + 1) * chunk) of the launch's tile list.  Euler: 8 CTAs per
+// SM (64 registers, 20 bytes spilled) measured 8 % faster than the 7 that
+// its unbounded 72 registers allow; Allaire is fastest unbounded.
 template <int MODEL>
-__global__ void __launch_bounds__(128) mixed_segment_x_kernel(MixedArgs A) {
+__global__ void __launch_bounds__(128, MODEL == MODEL_EULER ? 8 : 1)
+    mixed_segment_x_kernel(MixedArgs A) {
     const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int t_begin = gw * A.chunk;
     const int t_end = min(t_begin + A.chunk, A.ntiles);
