@@ -163,7 +163,9 @@ __device__ __forceinline__ void c2p_mixed(const Inst& I, const MPar& P, const fl
             p = fdiv(hi[4] - 0.5f * (hi[2] * u + hi[3] * v), eps);
         } else {
             // p = (rho e - kn) / eps with rho e = E - |M|^2 / (2 R) and
-            // kn = eps k, as one FP64 division: (E R - |M|^2/2 - kn R) / (R eps)
+            // kn = eps k, as (E R - |M|^2/2 - kn R) / (R eps): numerator and
+            // denominator in FP64 (the cancellation of p_inf happens in the
+            // numerator), the quotient in FP32, the precision of the result
             double R = ((double)hi[0] + (double)lo[0]) + ((double)hi[1] + (double)lo[1]);
             double M1 = (double)hi[2] + (double)lo[2], M2 = (double)hi[3] + (double)lo[3];
             double E = (double)hi[4] + (double)lo[4];
@@ -171,7 +173,7 @@ __device__ __forceinline__ void c2p_mixed(const Inst& I, const MPar& P, const fl
             double omz = 1.0 - zz;
             double eps = zz * I.pd[0] + omz * I.pd[1];
             double kn = zz * I.pd[2] + omz * I.pd[3];
-            p = (float)(((E * R - 0.5 * (M1 * M1 + M2 * M2)) - kn * R) / (R * eps));
+            p = fdiv((float)((E * R - 0.5 * (M1 * M1 + M2 * M2)) - kn * R), (float)(R * eps));
         }
         W[0] = hi[0];
         W[1] = hi[1];
