@@ -360,8 +360,9 @@ struct cfd_batch {
     };
     std::vector<Group> groups;
     bool dirty = true;
-    // [model][dir]; Euler y sweeps march by default (measured fastest on B200)
-    int shape[2][2] = {{0, kMarchShape}, {0, 0}};
+    // [model][dir]; y sweeps march by default (measured fastest on B200 for
+    // both models, and the strips adapt to the members)
+    int shape[2][2] = {{0, kMarchShape}, {0, kMarchShape}};
     int sms = 148;
     // graph of `graph_steps` ticks for the current membership
     cudaGraphExec_t graph = nullptr;

@@ -136,7 +136,7 @@ def test_autotune_keeps_results_and_picks_shapes():
     mem = _members()
     with G.Batch() as b:
         ids = [b.add(c, ic, 30) for c, ic, _ in mem]
-        ms = b.autotune(2)  # 2 x 3 shapes x 2 sweeps x 2 models steps of real work
+        ms = b.autotune(2)  # 2 steps x (1 x form + 4 y forms) x 2 models of real work
         assert ms > 0
         b.step(30)
         tuned = [b.download(i) for i in ids]
