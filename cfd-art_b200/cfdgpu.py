@@ -176,6 +176,8 @@ def lib() -> C.CDLL:
             "cfd_batch_autotune": (ip, [vp, ip, dp]),
             "cfd_batch_set_shapes": (ip, [vp, ip, ip, ip]),
             "cfd_batch_get_shapes": (ip, [vp, ip, C.POINTER(ip), C.POINTER(ip)]),
+            "cfd_batch_set_march_rows": (ip, [vp, ip, ip]),
+            "cfd_batch_get_march_rows": (ip, [vp, ip, C.POINTER(ip)]),
             "cfd_batch_status": (ip, [vp, ip, C.POINTER(Status)]),
             "cfd_batch_poll": (ip, [vp, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip), dp,
                                     C.POINTER(ip)]),
@@ -487,6 +489,15 @@ class Batch:
         check(lib().cfd_batch_get_shapes(self._h, model, C.byref(a), C.byref(b)),
               "cfd_batch_get_shapes")
         return a.value, b.value
+
+    def set_march_rows(self, model: int, rows: int) -> None:
+        """Strip length of the marching y sweep (16..64, 0 = chosen per tile list)."""
+        check(lib().cfd_batch_set_march_rows(self._h, model, rows), "cfd_batch_set_march_rows")
+
+    def march_rows(self, model: int) -> int:
+        r = C.c_int()
+        check(lib().cfd_batch_get_march_rows(self._h, model, C.byref(r)), "cfd_batch_get_march_rows")
+        return r.value
 
     def status(self, mid: int) -> Status:
         st = Status()

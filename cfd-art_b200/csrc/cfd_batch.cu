@@ -363,6 +363,8 @@ struct cfd_batch {
     // [model][dir]; y sweeps march by default (measured fastest on B200 for
     // both models, and the strips adapt to the members)
     int shape[2][2] = {{0, kMarchShape}, {0, kMarchShape}};
+    int march_fixed[2] = {0, 0};  // strip length set by the caller (0: chosen per tile list)
+    int march_used[2] = {0, 0};   // strip length of the current tile list
     int sms = 148;
     // graph of `graph_steps` ticks for the current membership
     cudaGraphExec_t graph = nullptr;
@@ -409,13 +411,18 @@ int build_tables(cfd_batch* b) {
     Shape shape_y[2];
     for (int model = 0; model < 2; ++model) {
         shape_y[model] = kShapesY[b->shape[model][DIR_Y]];
+        b->march_used[model] = 0;
         if (b->shape[model][DIR_Y] != kMarchShape) continue;
         std::vector<std::pair<int, int>> grids;
         for (const Member& m : b->members)
             if (m.cfg.model == model && !m.final) grids.emplace_back(m.cfg.nx, m.cfg.ny);
+        if (grids.empty()) continue;
         const int per_sm = model == CFD_MODEL_EULER ? march_per_sm<MODEL_EULER, DIR_Y>()
                                                     : march_per_sm<MODEL_ALLAIRE, DIR_Y>();
-        shape_y[model].ts = march_rows(grids, (long long)per_sm * b->sms * 4);
+        shape_y[model].ts = b->march_fixed[model]
+                                ? b->march_fixed[model]
+                                : march_rows(grids, (long long)per_sm * b->sms * 4);
+        b->march_used[model] = shape_y[model].ts;
     }
     std::vector<Inst> insts(b->members.size());
     for (size_t i = 0; i < b->members.size(); ++i) {
@@ -867,6 +874,22 @@ int cfd_batch_get_shapes(cfd_batch* b, int model, int* shape_x, int* shape_y) {
     if (!b || model < 0 || model > 1) return cfd_fail(CFD_ERR_INVALID, "bad arguments");
     if (shape_x) *shape_x = b->shape[model][DIR_X];
     if (shape_y) *shape_y = b->shape[model][DIR_Y];
+    return CFD_OK;
+}
+
+int cfd_batch_set_march_rows(cfd_batch* b, int model, int rows) {
+    if (!b || model < 0 || model > 1 || (rows != 0 && (rows < kMarchMinRows || rows > kMarchMaxRows)))
+        return cfd_fail(CFD_ERR_INVALID, "bad strip length (0 or %d..%d)", kMarchMinRows,
+                        kMarchMaxRows);
+    b->march_fixed[model] = rows;
+    b->dirty = true;
+    return CFD_OK;
+}
+
+int cfd_batch_get_march_rows(cfd_batch* b, int model, int* rows) {
+    if (!b || model < 0 || model > 1 || !rows) return cfd_fail(CFD_ERR_INVALID, "bad arguments");
+    if (int r = build_tables(b)) return r;
+    *rows = b->march_used[model];
     return CFD_OK;
 }
 

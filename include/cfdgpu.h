@@ -261,6 +261,13 @@ int cfd_batch_step_timed(cfd_batch* b, int ticks, double* ms_x, double* ms_y, in
 int cfd_batch_autotune(cfd_batch* b, int steps_per_trial, double* best_tick_ms);
 int cfd_batch_set_shapes(cfd_batch* b, int model, int shape_x, int shape_y);
 int cfd_batch_get_shapes(cfd_batch* b, int model, int* shape_x, int* shape_y);
+/* Strip length of the marching y sweep (y shape 3) of a model: rows in
+ * [16, 64], or 0 (default) to choose it for every tile list so that the
+ * strips fill the resident warps.  cfd_batch_get_march_rows reports the
+ * length the current tile list uses (0 when the model's y sweep does not
+ * march or the model has no active member).  Results do not depend on it. */
+int cfd_batch_set_march_rows(cfd_batch* b, int model, int rows);
+int cfd_batch_get_march_rows(cfd_batch* b, int model, int* rows);
 int cfd_batch_status(cfd_batch* b, int id, cfd_status* st);
 /* ids, steps taken, done flags and times of all members (cap entries). */
 int cfd_batch_poll(cfd_batch* b, int cap, int* ids, int* steps, int* done, double* t, int* count);

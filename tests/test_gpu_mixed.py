@@ -132,6 +132,37 @@ def test_tile_shapes_do_not_change_results():
             assert np.array_equal(outs[0][k], o[k])
 
 
+def test_march_strip_lengths_do_not_change_results():
+    """Marching strips of any length (the automatic choice, the shortest, an
+    odd one that leaves ragged last strips, the longest) give the tiles' bits;
+    lengths outside 16..64 are refused."""
+    mem = _members()
+    outs = {}
+    for rows in ("tiles", 0, 16, 37, 64):
+        with G.Batch() as b:
+            for model in (G.EULER, G.ALLAIRE):
+                if rows == "tiles":
+                    b.set_shapes(model, 0, 0)
+                else:
+                    b.set_shapes(model, 0, 3)
+                    b.set_march_rows(model, rows)
+            ids = [b.add(c, ic, 30) for c, ic, _ in mem]
+            if rows != "tiles":
+                for model in (G.EULER, G.ALLAIRE):
+                    used = b.march_rows(model)
+                    assert 16 <= used <= 64 and (rows == 0 or used == rows)
+            b.step(30)
+            outs[rows] = [b.download(i) for i in ids]
+    for rows in (0, 16, 37, 64):
+        for k in range(len(mem)):
+            assert np.array_equal(outs["tiles"][k], outs[rows][k]), (rows, k)
+    with G.Batch() as b:
+        for bad in (15, 65, -1):
+            with pytest.raises(G.CfdError):
+                b.set_march_rows(G.EULER, bad)
+        assert b.march_rows(G.ALLAIRE) == 0  # no members: no strips
+
+
 def test_autotune_keeps_results_and_picks_shapes():
     mem = _members()
     with G.Batch() as b:
