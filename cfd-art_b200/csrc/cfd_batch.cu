@@ -92,8 +92,8 @@ template <int MODEL, int DIR>
 int march_per_sm() {
     static int per_sm = 0;
     if (!per_sm) {
-        cudaError_t e =
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_march_kernel<MODEL, DIR>, 128, 0);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, mixed_march_kernel<MODEL, DIR>, 128, march_smem_bytes<MODEL>());
         if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     }
     return per_sm;
@@ -107,7 +107,7 @@ int launch_march(const MixedArgs& a, int sms, cudaStream_t st) {
     MixedArgs b = a;
     b.chunk = (a.ntiles + warps - 1) / warps;
     const int busy = (a.ntiles + b.chunk - 1) / b.chunk;
-    mixed_march_kernel<MODEL, DIR><<<(busy + 3) / 4, 128, 0, st>>>(b);
+    mixed_march_kernel<MODEL, DIR><<<(busy + 3) / 4, 128, march_smem_bytes<MODEL>(), st>>>(b);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "march launch: %s", cudaGetErrorString(e));
     return CFD_OK;
