@@ -151,11 +151,12 @@ int collect(cfd_server* s, Request* r) {
     return rc;
 }
 
-// The worker: admission, one round of steps for every admitted solve, then
-// completion.  Host work overlaps the round in flight: uploads of admitted
-// solves run on their own streams (the batch's copy stream, or each FP64
-// solve's stream), and the grids of solves found finished by the previous
-// round's status read are copied back while the next round runs.
+// The worker: one round of steps for every running solve, then completion.
+// Host work overlaps the round in flight: requests admitted before the round
+// are started (allocation and upload, on the batch's copy stream or on each
+// FP64 solve's stream) while it runs and join the next round, and the grids
+// of solves found finished by the previous round's status read are copied
+// back meanwhile.
 void worker_main(cfd_server* s) {
     cudaSetDevice(s->device);
     const int K = std::max(1, s->opt.ticks_per_round);
@@ -171,7 +172,35 @@ void worker_main(cfd_server* s) {
             if (s->stop) break;
             admit(s, start);
         }
+        std::vector<Request*> run;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            for (int64_t id : s->running) {
+                Request* r = s->reqs[id].get();
+                if (std::find(finished.begin(), finished.end(), r) == finished.end())
+                    run.push_back(r);
+            }
+            s->max_running = std::max<int>(s->max_running, (int)run.size());
+        }
+        auto tr = Clock::now();
+        // one round of steps (asynchronous)
+        if (!run.empty()) {
+            cudaEventRecord(s->ev0, s->stream);
+            if (mixed) {
+                if (cfd_batch_step(s->batch, K)) s->worker_error = CFD_ERR_CUDA;
+            } else {
+                for (Request* r : run) {
+                    cudaStreamWaitEvent(r->stream, s->ev0, 0);
+                    int k = std::min(K, r->steps - r->issued);
+                    if (k > 0 && cfd_advance(r->solver, k) == CFD_OK) r->issued += k;
+                    cudaEventRecord(r->ev, r->stream);
+                    cudaStreamWaitEvent(s->stream, r->ev, 0);
+                }
+            }
+            cudaEventRecord(s->ev1, s->stream);
+        }
         // start admitted requests (device allocation + upload, asynchronous)
+        // while the round runs; they join the next round
         for (Request* r : start) {
             int rc;
             if (mixed) {
@@ -201,33 +230,6 @@ void worker_main(cfd_server* s) {
                 s->running.push_back(r->id);
                 s->admitted++;
             }
-        }
-        std::vector<Request*> run;
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            for (int64_t id : s->running) {
-                Request* r = s->reqs[id].get();
-                if (std::find(finished.begin(), finished.end(), r) == finished.end())
-                    run.push_back(r);
-            }
-            s->max_running = std::max<int>(s->max_running, (int)run.size());
-        }
-        auto tr = Clock::now();
-        // one round of steps (asynchronous)
-        if (!run.empty()) {
-            cudaEventRecord(s->ev0, s->stream);
-            if (mixed) {
-                if (cfd_batch_step(s->batch, K)) s->worker_error = CFD_ERR_CUDA;
-            } else {
-                for (Request* r : run) {
-                    cudaStreamWaitEvent(r->stream, s->ev0, 0);
-                    int k = std::min(K, r->steps - r->issued);
-                    if (k > 0 && cfd_advance(r->solver, k) == CFD_OK) r->issued += k;
-                    cudaEventRecord(r->ev, r->stream);
-                    cudaStreamWaitEvent(s->stream, r->ev, 0);
-                }
-            }
-            cudaEventRecord(s->ev1, s->stream);
         }
         // grids of the solves the previous status read found finished, while
         // the round runs
