@@ -179,6 +179,9 @@ def lib() -> C.CDLL:
             "cfd_batch_set_march_rows": (ip, [vp, ip, ip]),
             "cfd_batch_get_march_rows": (ip, [vp, ip, C.POINTER(ip)]),
             "cfd_batch_status": (ip, [vp, ip, C.POINTER(Status)]),
+            "cfd_batch_poll_issue": (ip, [vp]),
+            "cfd_batch_poll_collect": (ip, [vp, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip), dp,
+                                        C.POINTER(ip)]),
             "cfd_batch_poll": (ip, [vp, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip), dp,
                                     C.POINTER(ip)]),
             "cfd_batch_download": (ip, [vp, ip, dp, ip]),
@@ -513,6 +516,22 @@ class Batch:
         cnt = C.c_int()
         check(lib().cfd_batch_poll(self._h, n, ids, steps, done, t, C.byref(cnt)), "cfd_batch_poll")
         return [(ids[i], steps[i], bool(done[i]), t[i]) for i in range(cnt.value)]
+
+    def poll_issue(self) -> None:
+        """Queues a status read behind the work queued so far (see poll_collect)."""
+        check(lib().cfd_batch_poll_issue(self._h), "cfd_batch_poll_issue")
+
+    def poll_collect(self):
+        """Waits for the read queued by poll_issue; entries as poll()."""
+        n = len(self.cfgs) + 1
+        ids = (C.c_int * n)()
+        steps = (C.c_int * n)()
+        done = (C.c_int * n)()
+        t = (C.c_double * n)()
+        cnt = C.c_int()
+        check(lib().cfd_batch_poll_collect(self._h, n, ids, steps, done, t, C.byref(cnt)),
+              "cfd_batch_poll_collect")
+        return [(ids[i], steps[i], bool(done[i]), t[i]) for i in range(min(cnt.value, n))]
 
     def download(self, mid: int, layout: int = GHOSTED_AOS,
                  out: np.ndarray | None = None) -> np.ndarray:

@@ -331,6 +331,17 @@ __global__ void gather_status(const Inst* __restrict__ insts, int n, PollRec* __
     out[i].done = st->done || st->n >= insts[i].max_steps;
 }
 
+// A status gather of every member queued on the batch stream and copied to
+// pinned memory; read once its event has completed.
+struct Gather {
+    PollRec* d = nullptr;
+    PollRec* h = nullptr;  // pinned
+    int cap = 0;
+    cudaEvent_t ev = nullptr;
+    bool pending = false;
+    std::vector<int> ids;  // member ids of the gathered entries
+};
+
 struct Member {
     bool final = false;   // seen done: later sweeps leave its state alone
     int id;
@@ -381,12 +392,9 @@ struct cfd_batch {
     int poll_cap = 0;
     // asynchronous status gather of cfd_batch_step (finished members leave
     // the tile lists without the host waiting for them)
-    PollRec* d_async = nullptr;
-    PollRec* h_async = nullptr;  // pinned
-    int async_cap = 0;
-    cudaEvent_t async_ev = nullptr;
-    bool async_pending = false;
-    std::vector<int> async_ids;  // member ids of the gathered entries
+    Gather async;
+    // the caller's two-phase status read (cfd_batch_poll_issue / _collect)
+    Gather issued;
 };
 
 namespace {
@@ -603,11 +611,13 @@ int cfd_batch_destroy(cfd_batch* b) {
     pool_free(b->d_insts, b->stream);
     pool_free(b->d_tiles, b->stream);
     pool_free(b->d_poll, b->stream);
-    pool_free(b->d_async, b->stream);
+    for (Gather* g : {&b->async, &b->issued}) pool_free(g->d, b->stream);
     cudaStreamSynchronize(b->stream);
     if (b->h_poll) cudaFreeHost(b->h_poll);
-    if (b->h_async) cudaFreeHost(b->h_async);
-    if (b->async_ev) cudaEventDestroy(b->async_ev);
+    for (Gather* g : {&b->async, &b->issued}) {
+        if (g->h) cudaFreeHost(g->h);
+        if (g->ev) cudaEventDestroy(g->ev);
+    }
     cudaStreamDestroy(b->copy);
     if (b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -945,14 +955,11 @@ int cfd_batch_autotune(cfd_batch* b, int steps_per_trial, double* best_ms) {
     return build_tables(b);
 }
 
-// Reads a completed asynchronous status gather (never waits) and takes the
-// members it found done out of the tile lists.
-static void take_async_status(cfd_batch* b) {
-    if (!b->async_pending || cudaEventQuery(b->async_ev) != cudaSuccess) return;
-    b->async_pending = false;
-    for (size_t i = 0; i < b->async_ids.size(); ++i) {
-        if (!b->h_async[i].done) continue;
-        Member* m = find(b, b->async_ids[i]);
+// Marks members a gather found done as finished: they leave the tile lists.
+static void mark_final(cfd_batch* b, const Gather& g) {
+    for (size_t i = 0; i < g.ids.size(); ++i) {
+        if (!g.h[i].done) continue;
+        Member* m = find(b, g.ids[i]);
         if (m && !m->final) {
             m->final = true;
             b->dirty = true;
@@ -960,35 +967,45 @@ static void take_async_status(cfd_batch* b) {
     }
 }
 
+// Reads a completed asynchronous status gather (never waits) and takes the
+// members it found done out of the tile lists.
+static void take_async_status(cfd_batch* b) {
+    if (!b->async.pending || cudaEventQuery(b->async.ev) != cudaSuccess) return;
+    b->async.pending = false;
+    mark_final(b, b->async);
+}
+
 // Queues a status gather of every member and its copy to pinned memory.
-static int issue_async_status(cfd_batch* b) {
+static int issue_gather(cfd_batch* b, Gather& g) {
     const int n = (int)b->members.size();
-    if (b->async_pending || n == 0) return CFD_OK;
-    if (!b->async_ev) BTRY(cudaEventCreateWithFlags(&b->async_ev, cudaEventDisableTiming));
-    if (n > b->async_cap) {
-        pool_free(b->d_async, b->stream);
-        b->d_async = nullptr;
-        if (b->h_async) {
+    if (g.pending || n == 0) return CFD_OK;
+    if (int r = build_tables(b)) return r;  // the device descriptors follow the membership
+    if (!g.ev) BTRY(cudaEventCreateWithFlags(&g.ev, cudaEventDisableTiming));
+    if (n > g.cap) {
+        pool_free(g.d, b->stream);
+        g.d = nullptr;
+        if (g.h) {
             BTRY(cudaStreamSynchronize(b->stream));
-            cudaFreeHost(b->h_async);
-            b->h_async = nullptr;
+            cudaFreeHost(g.h);
+            g.h = nullptr;
         }
         int c = std::max(64, 2 * n);
-        BTRY(pool_alloc(reinterpret_cast<void**>(&b->d_async), sizeof(PollRec) * c, b->stream));
-        BTRY(cudaHostAlloc(reinterpret_cast<void**>(&b->h_async), sizeof(PollRec) * c,
+        BTRY(pool_alloc(reinterpret_cast<void**>(&g.d), sizeof(PollRec) * c, b->stream));
+        BTRY(cudaHostAlloc(reinterpret_cast<void**>(&g.h), sizeof(PollRec) * c,
                            cudaHostAllocDefault));
-        b->async_cap = c;
+        g.cap = c;
     }
-    gather_status<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_insts, n, b->d_async);
+    gather_status<<<(n + 127) / 128, 128, 0, b->stream>>>(b->d_insts, n, g.d);
     BTRY(cudaGetLastError());
-    BTRY(cudaMemcpyAsync(b->h_async, b->d_async, sizeof(PollRec) * n, cudaMemcpyDeviceToHost,
-                         b->stream));
-    BTRY(cudaEventRecord(b->async_ev, b->stream));
-    b->async_ids.resize(n);
-    for (int i = 0; i < n; ++i) b->async_ids[i] = b->members[i].id;
-    b->async_pending = true;
+    BTRY(cudaMemcpyAsync(g.h, g.d, sizeof(PollRec) * n, cudaMemcpyDeviceToHost, b->stream));
+    BTRY(cudaEventRecord(g.ev, b->stream));
+    g.ids.resize(n);
+    for (int i = 0; i < n; ++i) g.ids[i] = b->members[i].id;
+    g.pending = true;
     return CFD_OK;
 }
+
+static int issue_async_status(cfd_batch* b) { return issue_gather(b, b->async); }
 
 int cfd_batch_step(cfd_batch* b, int ticks) {
     if (!b) return cfd_fail(CFD_ERR_INVALID, "null batch");
@@ -1105,6 +1122,32 @@ int cfd_batch_poll(cfd_batch* b, int cap, int* ids, int* steps, int* done, doubl
         if (b->h_poll[i].done) b->members[i].final = true;
         if (t) t[i] = b->h_poll[i].t;
     }
+    return CFD_OK;
+}
+
+int cfd_batch_poll_issue(cfd_batch* b) {
+    if (!b) return cfd_fail(CFD_ERR_INVALID, "null batch");
+    if (b->issued.pending) return cfd_fail(CFD_ERR_INVALID, "a status read is already issued");
+    return issue_gather(b, b->issued);
+}
+
+int cfd_batch_poll_collect(cfd_batch* b, int cap, int* ids, int* steps, int* done, double* t,
+                           int* count) {
+    if (!b || !count) return cfd_fail(CFD_ERR_INVALID, "null argument");
+    *count = 0;
+    Gather& g = b->issued;
+    if (!g.pending) return CFD_OK;
+    BTRY(cudaEventSynchronize(g.ev));
+    g.pending = false;
+    const int n = (int)g.ids.size();
+    *count = n;
+    for (int i = 0; i < n && i < cap; ++i) {
+        if (ids) ids[i] = g.ids[i];
+        if (steps) steps[i] = g.h[i].n;
+        if (done) done[i] = g.h[i].done;
+        if (t) t[i] = g.h[i].t;
+    }
+    mark_final(b, g);
     return CFD_OK;
 }
 

@@ -79,7 +79,7 @@ struct cfd_server {
     double cell_updates = 0.0;
     double busy_s = 0.0;
     double device_s = 0.0;   // CUDA-event time of the step rounds
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0[2] = {nullptr, nullptr}, ev1[2] = {nullptr, nullptr};  // round timing, two in flight
     int64_t completed = 0, rounds = 0, admitted = 0;
     int max_running = 0;
     int worker_error = 0;
@@ -155,19 +155,37 @@ int collect(cfd_server* s, Request* r) {
 // Host work overlaps the round in flight: requests admitted before the round
 // are started (allocation and upload, on the batch's copy stream or on each
 // FP64 solve's stream) while it runs and join the next round, and the grids
-// of solves found finished by the previous round's status read are copied
-// back meanwhile.
+// of finished solves are copied back meanwhile.  Mixed precision pipelines
+// the rounds: the status read queued after round r is collected while round
+// r+1 runs, so the GPU always has the next round queued (a solve found done
+// one round late has idled in that round; its result is unchanged).
 void worker_main(cfd_server* s) {
     cudaSetDevice(s->device);
     const int K = std::max(1, s->opt.ticks_per_round);
     const bool mixed = s->opt.precision == CFD_PREC_MIXED;
     std::vector<Request*> finished;  // found done, grids not yet collected
+    bool gather_pending = false;     // mixed: status read queued after the last round
+    std::vector<Request*> gathered;  // the solves that read covers
+    int slot = 0;                    // event pair of the round being launched
+    bool timed[2] = {false, false};
+    // device time of the round in event pair `sl` (waits for it)
+    auto account = [&](int sl) {
+        if (!timed[sl]) return;
+        float dev_ms = 0.f;
+        cudaEventSynchronize(s->ev1[sl]);
+        cudaEventElapsedTime(&dev_ms, s->ev0[sl], s->ev1[sl]);
+        timed[sl] = false;
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->device_s += 1e-3 * dev_ms;
+        s->rounds++;
+    };
     while (true) {
         std::vector<Request*> start;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait(lk, [&] {
-                return s->stop || !s->queue.empty() || !s->running.empty() || !finished.empty();
+                return s->stop || !s->queue.empty() || !s->running.empty() || !finished.empty() ||
+                       gather_pending;
             });
             if (s->stop) break;
             admit(s, start);
@@ -182,22 +200,23 @@ void worker_main(cfd_server* s) {
             }
             s->max_running = std::max<int>(s->max_running, (int)run.size());
         }
-        auto tr = Clock::now();
+        const auto t_iter = Clock::now();
         // one round of steps (asynchronous)
         if (!run.empty()) {
-            cudaEventRecord(s->ev0, s->stream);
+            cudaEventRecord(s->ev0[slot], s->stream);
             if (mixed) {
                 if (cfd_batch_step(s->batch, K)) s->worker_error = CFD_ERR_CUDA;
             } else {
                 for (Request* r : run) {
-                    cudaStreamWaitEvent(r->stream, s->ev0, 0);
+                    cudaStreamWaitEvent(r->stream, s->ev0[slot], 0);
                     int k = std::min(K, r->steps - r->issued);
                     if (k > 0 && cfd_advance(r->solver, k) == CFD_OK) r->issued += k;
                     cudaEventRecord(r->ev, r->stream);
                     cudaStreamWaitEvent(s->stream, r->ev, 0);
                 }
             }
-            cudaEventRecord(s->ev1, s->stream);
+            cudaEventRecord(s->ev1[slot], s->stream);
+            timed[slot] = true;
         }
         // start admitted requests (device allocation + upload, asynchronous)
         // while the round runs; they join the next round
@@ -231,30 +250,19 @@ void worker_main(cfd_server* s) {
                 s->admitted++;
             }
         }
-        // grids of the solves the previous status read found finished, while
-        // the round runs
-        for (Request* r : finished) {
-            int rc = collect(s, r);
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->running.erase(std::find(s->running.begin(), s->running.end(), r->id));
-            finish(s, r, rc);
-        }
-        if (!finished.empty()) s->cv_done.notify_all();
-        finished.clear();
-        if (run.empty()) continue;
-        // completion check: mixed, one gathered status read for the whole
-        // batch; FP64, a status read only for solves that may have finished
-        // (all steps issued, or a finite end time)
-        if (mixed) {
+        // mixed: the status read queued after the previous round (it waits
+        // for that round only; this round keeps the GPU busy meanwhile)
+        if (mixed && gather_pending) {
             int n = 0;
-            const int cap = (int)run.size() + 64;
+            const int cap = (int)gathered.size() + 64;
             std::vector<int> ids(cap), steps(cap), fin(cap);
             std::vector<double> tt(cap);
-            int rc = cfd_batch_poll(s->batch, cap, ids.data(), steps.data(), fin.data(), tt.data(),
-                                    &n);
+            int rc = cfd_batch_poll_collect(s->batch, cap, ids.data(), steps.data(), fin.data(),
+                                            tt.data(), &n);
+            gather_pending = false;
             std::map<int, int> pos;
             for (int i = 0; i < n && i < cap; ++i) pos[ids[i]] = i;
-            for (Request* r : run) {
+            for (Request* r : gathered) {
                 auto it = pos.find(r->member);
                 if (rc || it == pos.end()) {
                     finished.push_back(r);
@@ -269,7 +277,42 @@ void worker_main(cfd_server* s) {
                     finished.push_back(r);
                 }
             }
+            account(slot ^ 1);  // the previous round has completed
+        }
+        // grids of the finished solves, while the round runs
+        for (Request* r : finished) {
+            int rc = collect(s, r);
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->running.erase(std::find(s->running.begin(), s->running.end(), r->id));
+            finish(s, r, rc);
+        }
+        const bool collected = !finished.empty();
+        if (collected) s->cv_done.notify_all();
+        if (run.empty()) {
+            finished.clear();
+            account(slot ^ 1);
+            account(slot);
+            continue;
+        }
+        if (mixed) {
+            // the status after this round, collected during the next one
+            gathered.clear();
+            for (Request* r : run)
+                if (std::find(finished.begin(), finished.end(), r) == finished.end())
+                    gathered.push_back(r);
+            finished.clear();
+            if (!gathered.empty()) {
+                if (cfd_batch_poll_issue(s->batch)) {
+                    finished = gathered;  // the read failed: report them with their error
+                    gathered.clear();
+                } else {
+                    gather_pending = true;
+                }
+            }
         } else {
+            // completion check: a status read only for solves that may have
+            // finished (all steps issued, or a finite end time)
+            finished.clear();
             for (Request* r : run) {
                 if (r->issued < r->steps && std::isinf(r->cfg.T)) continue;
                 cfd_status st;
@@ -279,17 +322,16 @@ void worker_main(cfd_server* s) {
                     finished.push_back(r);
                 }
             }
+            account(slot);
         }
-        float dev_ms = 0.f;
-        cudaEventSynchronize(s->ev1);
-        cudaEventElapsedTime(&dev_ms, s->ev0, s->ev1);
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            s->busy_s += secs(tr, Clock::now());
-            s->device_s += 1e-3 * dev_ms;
-            s->rounds++;
+            s->busy_s += secs(t_iter, Clock::now());
         }
+        slot ^= 1;
     }
+    account(0);
+    account(1);
 }
 
 }  // namespace
@@ -342,8 +384,10 @@ int cfd_server_create(const cfd_server_options* opt, cfd_server** out) {
             return rc;
         }
     }
-    cudaEventCreate(&s->ev0);
-    cudaEventCreate(&s->ev1);
+    for (int i = 0; i < 2; ++i) {
+        cudaEventCreate(&s->ev0[i]);
+        cudaEventCreate(&s->ev1[i]);
+    }
     s->t0 = Clock::now();
     s->worker = std::thread(worker_main, s);
     *out = s;
@@ -454,8 +498,10 @@ int cfd_server_destroy(cfd_server* s) {
         if (r->ev) cudaEventDestroy(r->ev);
     }
     if (s->batch) cfd_batch_destroy(s->batch);
-    if (s->ev0) cudaEventDestroy(s->ev0);
-    if (s->ev1) cudaEventDestroy(s->ev1);
+    for (int i = 0; i < 2; ++i) {
+        if (s->ev0[i]) cudaEventDestroy(s->ev0[i]);
+        if (s->ev1[i]) cudaEventDestroy(s->ev1[i]);
+    }
     if (!s->opt.stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return CFD_OK;

@@ -271,6 +271,14 @@ int cfd_batch_get_march_rows(cfd_batch* b, int model, int* rows);
 int cfd_batch_status(cfd_batch* b, int id, cfd_status* st);
 /* ids, steps taken, done flags and times of all members (cap entries). */
 int cfd_batch_poll(cfd_batch* b, int cap, int* ids, int* steps, int* done, double* t, int* count);
+/* The same status read in two phases, for callers that queue the next steps
+ * before reading: _issue queues the gather behind the work queued so far and
+ * returns; _collect waits for that gather and returns what it saw, like
+ * cfd_batch_poll (members added after the issue are not in it; count = 0
+ * when nothing was issued).  One read may be outstanding at a time. */
+int cfd_batch_poll_issue(cfd_batch* b);
+int cfd_batch_poll_collect(cfd_batch* b, int cap, int* ids, int* steps, int* done, double* t,
+                           int* count);
 int cfd_batch_download(cfd_batch* b, int id, double* host, int layout);
 
 /* ---- continuous-batching server --------------------------------------------

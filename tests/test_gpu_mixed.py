@@ -163,6 +163,27 @@ def test_march_strip_lengths_do_not_change_results():
         assert b.march_rows(G.ALLAIRE) == 0  # no members: no strips
 
 
+def test_two_phase_status_read_matches_poll():
+    """poll_issue / poll_collect report what poll reports for the same point
+    of the stream, mark finished members, and refuse a second issue."""
+    mem = _members()[:3]
+    with G.Batch() as b:
+        ids = [b.add(c, ic, steps) for c, ic, steps in mem]
+        assert b.poll_collect() == []  # nothing issued
+        b.step(30)
+        b.poll_issue()
+        with pytest.raises(G.CfdError):
+            b.poll_issue()
+        got = b.poll_collect()
+        assert got == b.poll()
+        assert sorted(i for i, _, _, _ in got) == sorted(ids)
+        b.step(60)  # every member reaches its step limit
+        b.poll_issue()
+        got = b.poll_collect()
+        assert all(done for _, _, done, _ in got)
+        assert {i: n for i, n, _, _ in got} == {i: st for i, (_, _, st) in zip(ids, mem)}
+
+
 def test_autotune_keeps_results_and_picks_shapes():
     mem = _members()
     with G.Batch() as b:
