@@ -99,15 +99,12 @@ int march_per_sm() {
     return per_sm;
 }
 
-// Persistent marching y sweep (4-warp CTAs): as many warps as fit on the device, each
-// walking a contiguous range of strips.
+// Persistent marching y sweep (4-warp CTAs): as many warps as fit on the
+// device (never more than there are strips), each walking every W-th strip.
 template <int MODEL, int DIR>
 int launch_march(const MixedArgs& a, int sms, cudaStream_t st) {
     const int warps = std::max(1, std::min(a.ntiles, march_per_sm<MODEL, DIR>() * sms * 4));
-    MixedArgs b = a;
-    b.chunk = (a.ntiles + warps - 1) / warps;
-    const int busy = (a.ntiles + b.chunk - 1) / b.chunk;
-    mixed_march_kernel<MODEL, DIR><<<(busy + 3) / 4, 128, march_smem_bytes<MODEL>(), st>>>(b);
+    mixed_march_kernel<MODEL, DIR><<<(warps + 3) / 4, 128, march_smem_bytes<MODEL>(), st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "march launch: %s", cudaGetErrorString(e));
     return CFD_OK;
@@ -123,10 +120,7 @@ int launch_segment(const MixedArgs& a, int sms, cudaStream_t st) {
         if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     }
     const int warps = std::max(1, std::min(a.ntiles, per_sm * sms * 4));
-    MixedArgs b = a;
-    b.chunk = (a.ntiles + warps - 1) / warps;
-    const int busy = (a.ntiles + b.chunk - 1) / b.chunk;
-    mixed_segment_x_kernel<MODEL><<<(busy + 3) / 4, 128, 0, st>>>(b);
+    mixed_segment_x_kernel<MODEL><<<(warps + 3) / 4, 128, 0, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "segment launch: %s", cudaGetErrorString(e));
     return CFD_OK;
@@ -390,9 +384,10 @@ struct cfd_batch {
     PollRec* d_poll = nullptr;
     PollRec* h_poll = nullptr;  // pinned
     int poll_cap = 0;
-    // asynchronous status gather of cfd_batch_step (finished members leave
-    // the tile lists without the host waiting for them)
-    Gather async;
+    // asynchronous status gathers of cfd_batch_step, one per chunk of ticks
+    // in flight (finished members leave the tile lists one chunk later)
+    Gather async[2];
+    int async_next = 0;  // the slot the next chunk's gather uses
     // the caller's two-phase status read (cfd_batch_poll_issue / _collect)
     Gather issued;
 };
@@ -611,10 +606,10 @@ int cfd_batch_destroy(cfd_batch* b) {
     pool_free(b->d_insts, b->stream);
     pool_free(b->d_tiles, b->stream);
     pool_free(b->d_poll, b->stream);
-    for (Gather* g : {&b->async, &b->issued}) pool_free(g->d, b->stream);
+    for (Gather* g : {&b->async[0], &b->async[1], &b->issued}) pool_free(g->d, b->stream);
     cudaStreamSynchronize(b->stream);
     if (b->h_poll) cudaFreeHost(b->h_poll);
-    for (Gather* g : {&b->async, &b->issued}) {
+    for (Gather* g : {&b->async[0], &b->async[1], &b->issued}) {
         if (g->h) cudaFreeHost(g->h);
         if (g->ev) cudaEventDestroy(g->ev);
     }
@@ -967,12 +962,24 @@ static void mark_final(cfd_batch* b, const Gather& g) {
     }
 }
 
-// Reads a completed asynchronous status gather (never waits) and takes the
-// members it found done out of the tile lists.
-static void take_async_status(cfd_batch* b) {
-    if (!b->async.pending || cudaEventQuery(b->async.ev) != cudaSuccess) return;
-    b->async.pending = false;
-    mark_final(b, b->async);
+// Reads the asynchronous status gathers of cfd_batch_step and takes the
+// members they found done out of the tile lists: the one whose slot the
+// next chunk reuses is waited for (it follows the chunk before last, so the
+// last chunk keeps the GPU busy meanwhile and the host never runs more than
+// two chunks ahead); the other only if it has completed.
+static int take_async_status(cfd_batch* b) {
+    Gather& old = b->async[b->async_next];
+    if (old.pending) {
+        BTRY(cudaEventSynchronize(old.ev));
+        old.pending = false;
+        mark_final(b, old);
+    }
+    Gather& last = b->async[b->async_next ^ 1];
+    if (last.pending && cudaEventQuery(last.ev) == cudaSuccess) {
+        last.pending = false;
+        mark_final(b, last);
+    }
+    return CFD_OK;
 }
 
 // Queues a status gather of every member and its copy to pinned memory.
@@ -1005,7 +1012,11 @@ static int issue_gather(cfd_batch* b, Gather& g) {
     return CFD_OK;
 }
 
-static int issue_async_status(cfd_batch* b) { return issue_gather(b, b->async); }
+static int issue_async_status(cfd_batch* b) {
+    int r = issue_gather(b, b->async[b->async_next]);
+    b->async_next ^= 1;
+    return r;
+}
 
 int cfd_batch_step(cfd_batch* b, int ticks) {
     if (!b) return cfd_fail(CFD_ERR_INVALID, "null batch");
@@ -1014,7 +1025,7 @@ int cfd_batch_step(cfd_batch* b, int ticks) {
     const int kCheck = 64;      // ticks between status gathers
     int r;
     for (int done_ticks = 0; done_ticks < ticks;) {
-        take_async_status(b);
+        if ((r = take_async_status(b))) return r;
         if ((r = build_tables(b))) return r;
         if (b->groups.empty()) break;  // every member has finished
         const int chunk = std::min(kCheck, ticks - done_ticks);

@@ -413,14 +413,15 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
     }
 }
 
-// Persistent sweep: warp w of the grid walks the strips
-// [w * chunk, (w + 1) * chunk) of the launch's strip list.
+// Persistent sweep: warp w of the W warps of the grid walks the strips w,
+// w + W, w + 2W, ... of the launch's strip list, so the strips of members
+// that have finished (skipped) are spread over all warps instead of idling
+// some of them.
 template <int MODEL, int DIR>
 __global__ void __launch_bounds__(128) mixed_march_kernel(MixedArgs A) {
     const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int t_begin = gw * A.chunk;
-    const int t_end = min(t_begin + A.chunk, A.ntiles);
-    for (int tile = t_begin; tile < t_end; ++tile) {
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    for (int tile = gw; tile < A.ntiles; tile += nw) {
         const TileGeom g = tile_geom<DIR, kMarchMaxRows, 32>(A, tile);
         if (!g.skip) march_strip<MODEL, DIR>(A, g);
     }
@@ -579,17 +580,16 @@ __device__ __forceinline__ void segment_tile(const MixedArgs& A, const TileGeom&
     }
 }
 
-// Persistent x sweep: warp w of the grid walks the tiles
-// [w * chunk, (w + 1) * chunk) of the launch's tile list.  Euler: 8 CTAs per
+// Persistent x sweep: warp w of the W warps of the grid walks the tiles w,
+// w + W, w + 2W, ... of the launch's tile list.  Euler: 8 CTAs per
 // SM (64 registers, 20 bytes spilled) measured 8 % faster than the 7 that
 // its unbounded 72 registers allow; Allaire is fastest unbounded.
 template <int MODEL>
 __global__ void __launch_bounds__(128, MODEL == MODEL_EULER ? 8 : 1)
     mixed_segment_x_kernel(MixedArgs A) {
     const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int t_begin = gw * A.chunk;
-    const int t_end = min(t_begin + A.chunk, A.ntiles);
-    for (int tile = t_begin; tile < t_end; ++tile) {
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    for (int tile = gw; tile < A.ntiles; tile += nw) {
         const TileGeom g = tile_geom<DIR_X, kSegCells, kSegRows>(A, tile);
         if (!g.skip) segment_tile<MODEL>(A, g);
     }
