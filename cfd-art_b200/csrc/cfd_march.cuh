@@ -1,25 +1,29 @@
-// Mixed-precision sweeps by marching strips.
+// Barrier-free warp forms of the mixed-precision sweeps.
 //
-// A warp owns a strip of 32 lines x A.rows cells along the sweep of one
-// instance: lane = line, and every lane walks along its line one cell at a
-// time, keeping the last cells' primitive states, face states, raw cells and
-// flux in registers.  The strip length is chosen per launch on the host
-// (kMarchMinRows..kMarchMaxRows) so that the strips fill the resident warps.  The sweep therefore needs no shared memory and no barrier,
-// and re-reads only the two halo cells at each end of the strip.  In the y
-// sweep the lanes are 32 consecutive columns, so every step reads 32
-// consecutive cells (coalesced).  The code also has the x form (lanes on 32
-// rows, each lane reading consecutive cells of its row step by step), but
-// on B200 that form measured 1.9x slower than the tiled x sweep and its
-// contractions differ from the tiled ones, so the batch uses marching for y
-// only.  The arithmetic of every cell, face
-// and update is the one of the tiled sweep (cfd_mixed.cuh): the same
-// functions in the same order, so the two give the same results bit for bit
-// and the autotuner may pick either.
+// Marching strips (the y sweep): a warp owns a strip of 32 lines x A.rows
+// cells along the sweep of one instance: lane = line, and every lane walks
+// along its line one cell at a time, carrying the window the stencil needs
+// from one row to the next (primitive states, face states, raw cells, flux;
+// in registers, or for the six-component Allaire model partly in a per-lane
+// column of shared memory).  The strip length is chosen per launch on the
+// host (kMarchMinRows..kMarchMaxRows) so that the strips fill the resident
+// warps.  No barrier is needed, and only the two halo cells at each end of
+// a strip are re-read.  In the y sweep the lanes are 32 consecutive columns,
+// so every step reads 32 consecutive cells (coalesced).  The code also has
+// the x form (lanes on 32 rows, each lane reading consecutive cells of its
+// row step by step), but on B200 that form measured 1.9x slower than the
+// tiled x sweep, so the batch marches in y only.  The arithmetic of every
+// cell, face and update is the one of the tiled sweep (cfd_mixed.cuh): the
+// same functions in the same order, so the two give the same results bit for
+// bit and the autotuner may pick either.
 //
 // Reduction: each strip reduces its lanes' wave speeds and masses into its
 // own slot of the instance's partials; the strip that completes the
 // instance's ticket count combines the slots in slot order (reproducible
 // sums) and picks the instance's dt.
+//
+// Warp segments (the x sweep, further down): the lanes hold 32 consecutive
+// cells of a row and exchange neighbour values by shuffles.
 #pragma once
 
 #include "cfd_mixed.cuh"

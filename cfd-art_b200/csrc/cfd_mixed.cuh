@@ -7,9 +7,10 @@
 //     small increments are not lost to FP32 rounding step after step;
 //   * reconstruction, slope limiting, the half step and the HLLC solve in
 //     FP32 with hardware reciprocal / square-root approximations;
-//   * FP64 for the stiffened-gas pressure recovery p = rho e / eps - k of
-//     cells with pinf != 0 (pinf up to 6e8 cancels catastrophically in FP32),
-//     for the CFL wave-speed reduction and dt, and for the time accumulator.
+//   * FP64 for the numerator and denominator of the stiffened-gas pressure
+//     p = rho e / eps - k of cells with pinf != 0 (pinf up to 6e8 cancels
+//     catastrophically in FP32), for the sums of the CFL reduction, for dt
+//     and for the time accumulator.
 // The face states go to the Riemann solver as primitives, so the pressure
 // is never re-derived from a reconstructed FP32 energy.
 //
@@ -17,9 +18,10 @@
 // table maps blockIdx to (instance, tile); each instance has its own grid,
 // materials, options, buffers and device-resident time state, and its y
 // sweep finishes its own wave-speed reduction (last CTA of that instance).
-// The batch runs this tiled form for the y sweep (with the marching strips
-// of cfd_march.cuh as an alternative); the x sweep uses the warp segments of
-// cfd_march.cuh.  The tiled code is written for both directions.
+// The batch's y sweep marches strips by default (cfd_march.cuh) and offers
+// this tiled form as three alternative shapes with the same results; the x
+// sweep uses the warp segments of cfd_march.cuh.  The tiled code is written
+// for both directions, but only its y instantiations are launched.
 #pragma once
 
 #include "cfd_physics.cuh"
@@ -797,8 +799,8 @@ __device__ __forceinline__ void flush_run(const MixedArgs& A, int inst, int slot
 // Persistent sweep: a fixed grid of CTAs walks the tile list of every
 // instance in the launch; each thread loads its cell of the next tile while
 // the current tile is being computed.
-// Resident CTAs per SM: 4 for the Euler x sweep, 3 where the register need
-// is larger (the Euler y sweep with its reduction, every Allaire sweep).
+// Resident CTAs per SM: 3 for the y sweeps the batch launches (4 would suit
+// the Euler x form, which the batch does not launch).
 template <int MODEL, int DIR, int TS, int NA>
 __global__ void __launch_bounds__(256, (MODEL == MODEL_EULER && DIR == DIR_X) ? 4 : 3)
     mixed_sweep_kernel(MixedArgs A) {
