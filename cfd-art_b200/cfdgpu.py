@@ -134,6 +134,7 @@ def lib() -> C.CDLL:
             "cfd_upload_recipe": (ip, [vp, ip, C.c_uint64, ip, ip, C.c_double]),
             "cfd_upload_case": (ip, [vp, C.c_char_p, C.c_uint64, ip, C.c_double]),
             "cfd_download": (ip, [vp, dp, ip]),
+            "cfd_schlieren": (ip, [vp, ip, dp]),
             "cfd_compute_dt": (ip, [vp, ip, C.c_double, dp]),
             "cfd_step": (ip, [vp, C.c_double]),
             "cfd_advance": (ip, [vp, ip]),
@@ -158,6 +159,7 @@ def lib() -> C.CDLL:
             "cfd_recipe_ic": (ip, [cfgp, ip, C.c_uint64, ip, dp]),
             "cfd_write_state": (ip, [cfgp, dp, C.c_char_p, C.c_double]),
             "cfd_write_schlieren": (ip, [cfgp, dp, C.c_char_p, C.c_double]),
+            "cfd_write_schlieren_field": (ip, [cfgp, dp, C.c_char_p, C.c_double]),
             "cfd_write_masschange": (ip, [cfgp, C.c_char_p, ip, dp, dp, dp]),
             "cfd_write_lineout": (ip, [cfgp, dp, C.c_char_p, ip]),
             "cfd_read_settings": (ip, [C.c_char_p, C.POINTER(Settings)]),
@@ -327,6 +329,12 @@ class Solver:
             shape = c.ghosted_shape() if layout != SOA else (c.nvar, c.ny, c.nx)
             out = np.empty(shape)
         check(lib().cfd_download(self._h, _dp(out), layout), "cfd_download")
+        return out
+
+    def schlieren(self, ghosts: int = GHOSTED_AOS) -> np.ndarray:
+        """|grad rho| of every interior cell, computed on the device, (ny, nx)."""
+        out = np.empty((self.cfg.ny, self.cfg.nx))
+        check(lib().cfd_schlieren(self._h, ghosts, _dp(out)), "cfd_schlieren")
         return out
 
     def compute_dt(self, n: int, t: float) -> float:

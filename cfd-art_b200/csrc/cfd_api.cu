@@ -334,6 +334,54 @@ __global__ void soa_to_ghosted(const double* __restrict__ src, double* __restric
     }
 }
 
+// ---- schlieren field -------------------------------------------------------
+// |grad rho| by central differences at every interior cell, as the
+// reference's writer forms it (E/sourcecode/euler_io.cpp:1142-1185,
+// A/sourcecode/allaire_diffuse_io.cpp:1109-1150): gx = (rho_r - rho_l) /
+// (2 dx), gy = (rho_t - rho_b) / (2 dy), sqrt(gx^2 + gy^2), every operation
+// correctly rounded and none contracted, so the values equal the host
+// writer's.  An edge cell's outside neighbour is the boundary fill of the
+// current state (a mirror: the density of the edge cell itself) or, with
+// `frame`, the reference's ghost value.  Output row-major from the bottom
+// row, nx x ny.
+template <int MODEL>
+__device__ __forceinline__ double sch_rho(const double* __restrict__ src, long long plane,
+                                          long long off) {
+    return MODEL == MODEL_EULER ? src[off] : src[off] + src[plane + off];
+}
+
+template <int MODEL>
+__device__ __forceinline__ double sch_frame_rho(const double* __restrict__ frame, int gi, int gj,
+                                                int nx, int ny, int g, int nv) {
+    const double* fr = frame + frame_index(gi, gj, nx, ny, g) * nv;
+    return MODEL == MODEL_EULER ? fr[0] : fr[0] + fr[1];
+}
+
+template <int MODEL>
+__global__ void schlieren_field(const double* __restrict__ src, const double* __restrict__ frame,
+                                double* __restrict__ out, int nx, int ny, int g, int nv,
+                                int pitch, long long plane, double dx, double dy) {
+    const long long n = (long long)nx * ny;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx / nx), j = (int)(idx % nx);
+        const long long o = (long long)i * pitch + j;
+        const double rc = sch_rho<MODEL>(src, plane, o);
+        double rl, rr, rb, rt;
+        if (j > 0) rl = sch_rho<MODEL>(src, plane, o - 1);
+        else rl = frame ? sch_frame_rho<MODEL>(frame, i + g, g - 1, nx, ny, g, nv) : rc;
+        if (j < nx - 1) rr = sch_rho<MODEL>(src, plane, o + 1);
+        else rr = frame ? sch_frame_rho<MODEL>(frame, i + g, nx + g, nx, ny, g, nv) : rc;
+        if (i > 0) rb = sch_rho<MODEL>(src, plane, o - pitch);
+        else rb = frame ? sch_frame_rho<MODEL>(frame, g - 1, j + g, nx, ny, g, nv) : rc;
+        if (i < ny - 1) rt = sch_rho<MODEL>(src, plane, o + pitch);
+        else rt = frame ? sch_frame_rho<MODEL>(frame, ny + g, j + g, nx, ny, g, nv) : rc;
+        const double gx = (rr - rl) / (2.0 * dx);
+        const double gy = (rt - rb) / (2.0 * dy);
+        out[idx] = sqrt(gx * gx + gy * gy);
+    }
+}
+
 // ---- reference ghost values --------------------------------------------------
 // The reference's grid keeps its ghost cells between boundary fills: after
 // set_ICs they hold the initial condition's own values, later the fill that
@@ -829,6 +877,34 @@ int cfd_download(cfd_solver* s, double* host, int layout) {
     } else {
         return fail(CFD_ERR_INVALID, "unknown layout %d", layout);
     }
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return CFD_OK;
+}
+
+int cfd_schlieren(cfd_solver* s, int ghosts, double* host) {
+    if (!s || !host) return fail(CFD_ERR_INVALID, "null argument");
+    if (!s->uploaded) return fail(CFD_ERR_STATE, "no state uploaded");
+    if (ghosts != CFD_LAYOUT_GHOSTED_AOS && ghosts != CFD_LAYOUT_GHOSTED_AOS_AS_REFERENCE)
+        return fail(CFD_ERR_INVALID, "ghosts: CFD_LAYOUT_GHOSTED_AOS or _AS_REFERENCE");
+    const double* frame = nullptr;
+    if (ghosts == CFD_LAYOUT_GHOSTED_AOS_AS_REFERENCE) {
+        if (!s->frame)
+            return fail(CFD_ERR_STATE, "reference ghost values are off (cfd_set_reference_ghosts)");
+        frame = s->frame;
+    }
+    const cfd_config& c = s->cfg;
+    int cur, r;
+    if ((r = current_buffer(s, cur))) return r;
+    double* out = s->buf[cur ^ 1];  // scratch: the other state buffer
+    if (c.model == CFD_MODEL_EULER)
+        schlieren_field<MODEL_EULER><<<148 * 8, 256, 0, s->stream>>>(
+            s->buf[cur], frame, out, c.nx, c.ny, s->g, s->nv, s->pitch, s->plane, c.dx, c.dy);
+    else
+        schlieren_field<MODEL_ALLAIRE><<<148 * 8, 256, 0, s->stream>>>(
+            s->buf[cur], frame, out, c.nx, c.ny, s->g, s->nv, s->pitch, s->plane, c.dx, c.dy);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(host, out, sizeof(double) * c.nx * (size_t)c.ny,
+                             cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return CFD_OK;
 }

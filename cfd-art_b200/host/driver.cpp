@@ -57,6 +57,13 @@ int main(int argc, char** argv) {
         schlieren_times = {0.000115, 0.000175, 0.000247, 0.000307, 0.000378, 0.000402, 0.000477,
                            0.001080};
     bool have = false;  // grid holds the state of this output call
+    // schlieren frames: |grad rho| formed on the device, nx*ny values copied back
+    std::vector<double> field((size_t)cfg.nx * cfg.ny);
+    auto schlieren = [&](double t) -> int {
+        int r = cfd_schlieren(s, CFD_LAYOUT_GHOSTED_AOS_AS_REFERENCE, field.data());
+        if (!r) r = cfd_write_schlieren_field(&cfg, field.data(), base.c_str(), t);
+        return r;
+    };
     auto fetch = [&]() -> int {
         if (have) return 0;
         have = true;
@@ -66,8 +73,7 @@ int main(int argc, char** argv) {
         have = false;
         int r;
         if (!schlieren_times.empty() && t > schlieren_times[0]) {
-            if ((r = fetch())) return r;
-            cfd_write_schlieren(&cfg, grid.data(), base.c_str(), t);
+            if ((r = schlieren(t))) return r;
             schlieren_times.erase(schlieren_times.begin());
         }
         bool final_out = (t == T);
@@ -76,7 +82,7 @@ int main(int argc, char** argv) {
         if (!due) return 0;
         if ((r = fetch())) return r;
         cfd_write_state(&cfg, grid.data(), base.c_str(), t);
-        cfd_write_schlieren(&cfg, grid.data(), base.c_str(), t);
+        if ((r = schlieren(t))) return r;
         if (allaire && (n == 0 || final_out)) cfd_write_lineout(&cfg, grid.data(), base.c_str(), n);
         if (final_out && !tt.empty())
             cfd_write_masschange(&cfg, base.c_str(), (int)tt.size(), tt.data(), m1.data(), m2.data());

@@ -201,13 +201,22 @@ int cfd_write_schlieren(const cfd_config* c, const double* grid, const char* bas
             double gy = (rt - rb) / (2.0 * v.dy);
             g.push_back(std::sqrt(gx * gx + gy * gy));
         }
-    double mx = *std::max_element(g.begin(), g.end());
+    return cfd_write_schlieren_field(c, g.data(), basename, t);
+}
+
+int cfd_write_schlieren_field(const cfd_config* c, const double* field, const char* basename,
+                              double t) {
+    if (!c || !field || !basename) return CFD_ERR_INVALID;
+    const size_t n = (size_t)c->nx * c->ny;
+    double mx = *std::max_element(field, field + n);
     std::ofstream out(std::string(basename) + "-schlieren-" + std::to_string(t) + ".dat");
     if (!out) return CFD_ERR_INVALID;
     size_t k = 0;
-    for (int i = v.g; i < v.ny + v.g; ++i) {
-        for (int j = v.g; j < v.nx + v.g; ++j) {
-            out << v.ccx(j) << " " << v.ccy(i) << " " << g[k] / mx << std::endl;
+    for (int i = 0; i < c->ny; ++i) {
+        const double y = c->y0 + double(i) * c->dy + 0.5 * c->dy;  // cell centres as View
+        for (int j = 0; j < c->nx; ++j) {
+            const double x = c->x0 + double(j) * c->dx + 0.5 * c->dx;
+            out << x << " " << y << " " << field[k] / mx << std::endl;
             ++k;
         }
         out << std::endl;

@@ -133,6 +133,17 @@ int cfd_upload_case(cfd_solver* s, const char* test_case, uint64_t seed, int n, 
 /* Copies the current state to the host in `layout`.  In the ghosted layout
  * the ghost strips hold the boundary fill of the current state. */
 int cfd_download(cfd_solver* s, double* host, int layout);
+/* Schlieren field of the current state computed on the device: |grad rho|
+ * of every interior cell by central differences, as the reference's writer
+ * forms it (E/sourcecode/euler_io.cpp:1142-1185, A/sourcecode/
+ * allaire_diffuse_io.cpp:1109-1150), the same values as the host writer's,
+ * nx*ny doubles from the bottom row up.  `ghosts` picks the outside
+ * neighbours of edge cells like cfd_download's layouts:
+ * CFD_LAYOUT_GHOSTED_AOS (boundary fill of the current state) or
+ * CFD_LAYOUT_GHOSTED_AOS_AS_REFERENCE (the reference's ghost values).  Only
+ * nx*ny doubles cross to the host instead of the ghosted grid;
+ * cfd_write_schlieren_field normalises and writes them. */
+int cfd_schlieren(cfd_solver* s, int ghosts, double* host);
 
 /* Checkpoint / resume.  cfd_checkpoint_save writes the current state, the
  * device time-loop state (n, t, the dt chosen for the next step, wave speeds,

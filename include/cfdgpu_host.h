@@ -81,6 +81,11 @@ int cfd_settings_ic(const cfd_settings* s, const cfd_config* cfg, double* grid);
  * with <t> formatted like std::to_string(double). */
 int cfd_write_state(const cfd_config* cfg, const double* grid, const char* basename, double t);
 int cfd_write_schlieren(const cfd_config* cfg, const double* grid, const char* basename, double t);
+/* The schlieren file from a field of |grad rho| values (nx*ny, bottom row
+ * first; cfd_schlieren computes it on the device): normalised by its
+ * maximum and written exactly as cfd_write_schlieren writes it. */
+int cfd_write_schlieren_field(const cfd_config* cfg, const double* field, const char* basename,
+                              double t);
 /* Allaire lineouts <basename>-lineoutx-<n>.dat and -lineouty-<n>.dat: row
  * Ny/2 and column Nx/2 of the ghosted grid, ghost cells included
  * (A/sourcecode/allaire_diffuse_io.cpp:1188-1232). */

@@ -96,3 +96,32 @@ def test_reference_ghosts_enabled_after_steps_and_disabled():
         with pytest.raises(G.CfdError):
             s.download(G.GHOSTED_AOS_AS_REFERENCE)
         s.advance(16)  # recaptured graph without the frame still runs
+
+
+def _schlieren_host(grid, model, dx, dy, g):
+    """|grad rho| of the interior cells of a ghosted AoS grid, formed as the
+    host writer forms it."""
+    rho = grid[..., 0] if model == G.EULER else grid[..., 0] + grid[..., 1]
+    gx = (rho[g:-g, g + 1:rho.shape[1] - g + 1] - rho[g:-g, g - 1:-g - 1]) / (2.0 * dx)
+    gy = (rho[g + 1:rho.shape[0] - g + 1, g:-g] - rho[g - 1:-g - 1, g:-g]) / (2.0 * dy)
+    return np.sqrt(gx * gx + gy * gy)
+
+
+@pytest.mark.parametrize("model,case,nx,ny,opt,steps", CASES)
+def test_device_schlieren_equals_host(model, case, nx, ny, opt, steps):
+    """The schlieren field computed on the device equals the one formed from
+    the downloaded grid, bit for bit, with either kind of ghost values."""
+    cfg = _config(model, case, nx, ny, opt)
+    ic = G.case_ic(cfg, case)
+    g = 1 if opt.get("flux_solver") == "Godunov" else 2
+    with G.Solver(cfg) as s:
+        s.set_reference_ghosts(True)
+        s.upload(ic)
+        s.advance(steps)
+        for layout in (G.GHOSTED_AOS, G.GHOSTED_AOS_AS_REFERENCE):
+            host = _schlieren_host(s.download(layout), model, cfg.dx, cfg.dy, g)
+            dev = s.schlieren(layout)
+            assert dev.shape == host.shape
+            assert np.array_equal(dev, host), layout
+        with pytest.raises(G.CfdError):
+            s.schlieren(G.SOA)

@@ -155,6 +155,15 @@ def test_invalid_configs_rejected_without_touching_a_device():
         assert G.last_error()
 
 
+def _schlieren_field(grid, model, dx, dy, g=2):
+    """|grad rho| of the interior cells of a ghosted AoS grid by central
+    differences, each operation as the writers form it."""
+    rho = grid[..., 0] if model == "euler" else grid[..., 0] + grid[..., 1]
+    gx = (rho[g:-g, g + 1:rho.shape[1] - g + 1] - rho[g:-g, g - 1:-g - 1]) / (2.0 * dx)
+    gy = (rho[g + 1:rho.shape[0] - g + 1, g:-g] - rho[g - 1:-g - 1, g:-g]) / (2.0 * dy)
+    return np.ascontiguousarray(np.sqrt(gx * gx + gy * gy))
+
+
 @pytest.mark.skipif(not O.ref_available("euler"), reason="reference build absent")
 @pytest.mark.parametrize("model,case", [("euler", "cross"), ("allaire", "ST2_x")])
 def test_output_writers_match_reference(tmp_path, model, case):
@@ -173,6 +182,13 @@ def test_output_writers_match_reference(tmp_path, model, case):
         b = tmp_path / f"ours-{kind}-0.012346.dat"
         assert a.exists() and b.exists()
         assert filecmp.cmp(a, b, shallow=False), kind
+    # the field writer (used with the device-computed field) writes the same
+    # file from |grad rho| formed the same way
+    field = _schlieren_field(grid, model, cfg.dx, cfg.dy)
+    fp = field.ctypes.data_as(C.POINTER(C.c_double))
+    assert L.cfd_write_schlieren_field(C.byref(cfg), fp, str(tmp_path / "field").encode(), t) == 0
+    assert filecmp.cmp(tmp_path / "ref-schlieren-0.012346.dat",
+                       tmp_path / "field-schlieren-0.012346.dat", shallow=False)
     if model == "allaire":
         assert L.cfd_write_lineout(C.byref(cfg), gp, str(tmp_path / "ours").encode(), 5) == 0
         for kind in ("lineoutx", "lineouty"):
