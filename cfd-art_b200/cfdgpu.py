@@ -92,7 +92,7 @@ class Settings(C.Structure):
 class ServerOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("budget_bytes", C.c_size_t),
                 ("budget_fraction", C.c_double), ("ticks_per_round", C.c_int),
-                ("stream", C.c_void_p)]
+                ("stream", C.c_void_p), ("host_pinned_bytes", C.c_size_t)]
 
 
 class RequestInfo(C.Structure):
@@ -556,9 +556,9 @@ class Server:
     thread, wait for their final grids; a worker thread owns the GPU."""
 
     def __init__(self, precision: int = MIXED, budget_bytes: int = 0, budget_fraction: float = 0.8,
-                 ticks_per_round: int = 16, stream: int | None = None):
+                 ticks_per_round: int = 16, stream: int | None = None, host_pinned_bytes: int = 0):
         o = ServerOptions(precision, budget_bytes, budget_fraction, ticks_per_round,
-                          C.c_void_p(stream) if stream else None)
+                          C.c_void_p(stream) if stream else None, host_pinned_bytes)
         h = C.c_void_p()
         check(lib().cfd_server_create(C.byref(o), C.byref(h)), "cfd_server_create")
         self._h = h

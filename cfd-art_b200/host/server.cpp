@@ -39,10 +39,80 @@ double secs(Clock::time_point a, Clock::time_point b) {
     return std::chrono::duration<double>(b - a).count();
 }
 
+// Pinned host memory for request grids, carved first-fit out of one
+// allocation made when the server starts (pinning is slow; reuse is free).
+// Callers hold the server lock.
+class PinnedArena {
+    char* base_ = nullptr;
+    std::map<size_t, size_t> free_;  // offset -> bytes, coalesced
+ public:
+    bool init(size_t bytes) {
+        if (!bytes || cudaHostAlloc(reinterpret_cast<void**>(&base_), bytes,
+                                    cudaHostAllocDefault) != cudaSuccess) {
+            base_ = nullptr;
+            return false;
+        }
+        free_[0] = bytes;
+        return true;
+    }
+    ~PinnedArena() {
+        if (base_) cudaFreeHost(base_);
+    }
+    static size_t round(size_t bytes) { return (bytes + 255) / 256 * 256; }
+    double* alloc(size_t bytes) {
+        if (!base_) return nullptr;
+        bytes = round(bytes);
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            const size_t off = it->first, left = it->second - bytes;
+            free_.erase(it);
+            if (left) free_[off + bytes] = left;
+            return reinterpret_cast<double*>(base_ + off);
+        }
+        return nullptr;
+    }
+    void release(double* p, size_t bytes) {
+        size_t off = reinterpret_cast<char*>(p) - base_;
+        bytes = round(bytes);
+        auto next = free_.lower_bound(off);
+        if (next != free_.end() && off + bytes == next->first) {
+            bytes += next->second;
+            next = free_.erase(next);
+        }
+        if (next != free_.begin()) {
+            auto prev = std::prev(next);
+            if (prev->first + prev->second == off) {
+                prev->second += bytes;
+                return;
+            }
+        }
+        free_[off] = bytes;
+    }
+};
+
 struct Request {
     int64_t id;
     cfd_config cfg;
-    std::vector<double> ic;   // ghosted AoS initial grid; reused for the result
+    // ghosted AoS initial grid, reused for the result: in the server's pinned
+    // arena when it had room, else in `own`
+    double* grid = nullptr;
+    size_t elems = 0;
+    std::vector<double> own;
+    PinnedArena* arena = nullptr;  // owner of `grid` when pinned
+    ~Request() {
+        if (arena && grid) arena->release(grid, elems * sizeof(double));
+    }
+    // room for `n` doubles (pinned when the arena has it)
+    void place(PinnedArena* a, size_t n) {
+        elems = n;
+        grid = a ? a->alloc(n * sizeof(double)) : nullptr;
+        if (grid) {
+            arena = a;
+        } else {
+            own.resize(n);
+            grid = own.data();
+        }
+    }
     int recipe = 0;           // > 0: initial condition built on the device at admission
     uint64_t seed = 0;
     int nbubbles = 0;
@@ -66,6 +136,7 @@ struct cfd_server {
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<int64_t> queue;
+    PinnedArena arena;  // request grids (under mu); declared first, destroyed after reqs
     std::map<int64_t, std::unique_ptr<Request>> reqs;
     std::vector<int64_t> running;
     int64_t next_id = 1;
@@ -130,17 +201,18 @@ void finish(cfd_server* s, Request* r, int err) {
 
 // Returns a finished request's grid to it and releases its device state.
 int collect(cfd_server* s, Request* r) {
-    if (r->ic.empty()) {  // device-built initial condition: room for the result
+    if (!r->grid) {  // device-built initial condition: room for the result
         size_t elems = 0;
         cfd_ic_grid_elems(&r->cfg, &elems);
-        r->ic.resize(elems);
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->place(&s->arena, elems);
     }
     int rc;
     if (s->opt.precision == CFD_PREC_MIXED) {
-        rc = cfd_batch_download(s->batch, r->member, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS);
+        rc = cfd_batch_download(s->batch, r->member, r->grid, CFD_LAYOUT_GHOSTED_AOS);
         cfd_batch_remove(s->batch, r->member);
     } else {
-        rc = cfd_download(r->solver, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS);
+        rc = cfd_download(r->solver, r->grid, CFD_LAYOUT_GHOSTED_AOS);
         cfd_destroy(r->solver);
         r->solver = nullptr;
         cudaStreamDestroy(r->stream);
@@ -225,7 +297,7 @@ void worker_main(cfd_server* s) {
             if (mixed) {
                 rc = r->recipe ? cfd_batch_add_recipe(s->batch, &r->cfg, r->recipe, r->seed,
                                                       r->nbubbles, r->steps, &r->member)
-                               : cfd_batch_add(s->batch, &r->cfg, r->ic.data(), r->steps,
+                               : cfd_batch_add(s->batch, &r->cfg, r->grid, r->steps,
                                                &r->member);
             } else {
                 cfd_config c = r->cfg;
@@ -238,7 +310,7 @@ void worker_main(cfd_server* s) {
                 if (!rc)
                     rc = r->recipe ? cfd_upload_recipe(r->solver, r->recipe, r->seed, r->nbubbles,
                                                        0, 0.0)
-                                   : cfd_upload(r->solver, r->ic.data(), CFD_LAYOUT_GHOSTED_AOS,
+                                   : cfd_upload(r->solver, r->grid, CFD_LAYOUT_GHOSTED_AOS,
                                                 0, 0.0);
             }
             std::lock_guard<std::mutex> lk(s->mu);
@@ -345,8 +417,13 @@ int enqueue(cfd_server* s, std::unique_ptr<Request> r, int64_t* id_out) {
     if (s->opt.precision == CFD_PREC_MIXED) cfd_batch_member_bytes(cfg, &need);
     else need = fp64_bytes(*cfg);
     std::lock_guard<std::mutex> lk(s->mu);
-    if (need > s->budget)
+    if (need > s->budget) {
+        if (r->arena) {  // give the grid back while holding the lock
+            r->arena->release(r->grid, r->elems * sizeof(double));
+            r->arena = nullptr;
+        }
         return cfd_fail(CFD_ERR_BUDGET, "request needs %zu bytes, the budget is %zu", need, s->budget);
+    }
     r->id = s->next_id++;
     *id_out = r->id;
     s->queue.push_back(r->id);
@@ -388,6 +465,7 @@ int cfd_server_create(const cfd_server_options* opt, cfd_server** out) {
         cudaEventCreate(&s->ev0[i]);
         cudaEventCreate(&s->ev1[i]);
     }
+    if (opt->host_pinned_bytes) s->arena.init(opt->host_pinned_bytes);  // pageable if it fails
     s->t0 = Clock::now();
     s->worker = std::thread(worker_main, s);
     *out = s;
@@ -402,7 +480,11 @@ int cfd_server_submit(cfd_server* s, const cfd_config* cfg, const double* ic, in
     auto r = std::make_unique<Request>();
     r->cfg = *cfg;
     r->cfg.stream = nullptr;
-    r->ic.assign(ic, ic + elems);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->place(&s->arena, elems);
+    }
+    memcpy(r->grid, ic, elems * sizeof(double));  // outside the lock
     r->steps = steps;
     return enqueue(s, std::move(r), id_out);
 }
@@ -448,7 +530,7 @@ int cfd_server_wait(cfd_server* s, int64_t id, double timeout_s, cfd_request_inf
         info->latency_s = secs(r->t_submit, r->t_done);
         info->submit_s = secs(s->t0, r->t_submit);
     }
-    if (result && r->state == CFD_REQ_DONE) memcpy(result, r->ic.data(), r->ic.size() * sizeof(double));
+    if (result && r->state == CFD_REQ_DONE) memcpy(result, r->grid, r->elems * sizeof(double));
     return r->state == CFD_REQ_FAILED ? cfd_fail(r->error, "request %lld failed", (long long)id)
                                       : CFD_OK;
 }

@@ -307,6 +307,9 @@ typedef struct cfd_server_options {
     double budget_fraction; /* of the free device memory at creation (0: 0.8) */
     int ticks_per_round;    /* steps between admission points (0: 16) */
     void* stream;           /* cudaStream_t for all work (NULL: the server creates one) */
+    size_t host_pinned_bytes; /* pinned host arena for request grids (0: none): a request
+                               * placed there is uploaded and read back without staging,
+                               * so the worker keeps the GPU fed; others use pageable memory */
 } cfd_server_options;
 
 typedef struct cfd_request_info {

@@ -104,3 +104,26 @@ def test_submissions_from_many_threads():
         for i, n in ids:
             info, _ = srv.wait(i, want_result=False)
             assert info.state == G.REQ_DONE and info.steps == n
+
+
+@pytest.mark.parametrize("precision", [G.MIXED, G.FP64])
+def test_pinned_arena_gives_the_same_results(precision):
+    """Request grids in the server's pinned host arena (room for about two at
+    a time here, so later requests reuse freed room and the rest fall back to
+    pageable memory) give the results of a server without one."""
+    reqs = _requests()
+    room = 2 * max(ic.nbytes for _, ic, _ in reqs)
+    outs = {}
+    for pinned in (0, room):
+        with G.Server(precision, ticks_per_round=6, host_pinned_bytes=pinned) as srv:
+            got = []
+            for _ in range(2):  # the second pass reuses arena room the first released
+                ids = [srv.submit(c, ic, n) for c, ic, n in reqs]
+                got.append([srv.wait(i)[1] for i in ids])
+                for i in ids:
+                    srv.release(i)
+            outs[pinned] = got
+    for a, b in zip(outs[0][0], outs[room][0]):
+        assert np.array_equal(a, b)
+    for a, b in zip(outs[room][0], outs[room][1]):
+        assert np.array_equal(a, b)
