@@ -6,6 +6,8 @@ Two oracles live under ``oracle/``:
   C++ sources (euler_equations/euler_simulation_code, allaire_2d) compiled
   against the Eigen-subset shim plus the hook drivers ``ref_*_hook.cpp``.
 * ``_build/liboracle.so``: the plain-C restatement ``cfd_oracle.c``.
+* ``_build/libopcount.so``: the same restatement compiled with a counting
+  double (``opcount.cpp``), for exact operation counts per cell-update.
 
 Only the tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline /
 reference arm import this module.  The shipped library never does.
@@ -235,12 +237,73 @@ def port_compute_dt(model: str, p: RefParams, grid: np.ndarray, n: int, t: float
     return dt, mass
 
 
+# --------------------------------------------------------------------------
+# counted restatement (opcount.cpp)
+
+OP_CATEGORIES = ("add", "mul", "div", "sqrt", "cmp", "sign")
+OP_PHASES = ("dt", "step", "other")
+
+
+def opcount_lib() -> C.CDLL:
+    lib = _load("opcount", PORT_DIR / "libopcount.so")
+    u64p = C.POINTER(C.c_uint64)
+    lib.opcount_run.restype = C.c_int
+    lib.opcount_run.argtypes = [C.c_int, C.POINTER(RefParams), C.POINTER(C.c_double), C.c_int,
+                                C.POINTER(C.c_int), C.POINTER(C.c_double), u64p]
+    lib.opcount_face.restype = None
+    lib.opcount_face.argtypes = [C.c_int, C.POINTER(RefParams), C.POINTER(C.c_double),
+                                 C.c_double, C.c_double, C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double), C.POINTER(C.c_double), u64p]
+    nc, nph = C.c_int(), C.c_int()
+    lib.opcount_layout(C.byref(nc), C.byref(nph))
+    if (nc.value, nph.value) != (len(OP_CATEGORIES), len(OP_PHASES)):
+        raise RuntimeError("libopcount.so count layout differs from oracle_py")
+    return lib
+
+
+def _counts_dict(raw: np.ndarray) -> dict[str, dict[str, int]]:
+    m = raw.reshape(len(OP_PHASES), len(OP_CATEGORIES))
+    return {ph: {c: int(m[i, j]) for j, c in enumerate(OP_CATEGORIES)}
+            for i, ph in enumerate(OP_PHASES)}
+
+
+def opcount_run(model: str, p: RefParams, grid: np.ndarray, max_steps: int, n: int = 0,
+                t: float = 0.0):
+    """Counted time loop (same states as port_run, grid advanced in place).
+
+    Returns (steps_taken, n, t, counts) with counts[phase][category] totals
+    over the run; phases "dt" (compute_dt) and "step" (the split update)."""
+    lib = opcount_lib()
+    raw = np.zeros(len(OP_PHASES) * len(OP_CATEGORIES), dtype=np.uint64)
+    nn = C.c_int(n)
+    tt = C.c_double(t)
+    taken = lib.opcount_run(MODEL_ID[model], C.byref(p), _dptr(grid), int(max_steps),
+                            C.byref(nn), C.byref(tt), raw.ctypes.data_as(C.POINTER(C.c_uint64)))
+    if taken < 0:
+        raise MemoryError("opcount_run could not allocate its grids")
+    return taken, nn.value, tt.value, _counts_dict(raw)
+
+
+def opcount_face(model: str, p: RefParams, stencil: np.ndarray, dt: float, dx: float):
+    """Counted single face: (flux, u_star, z_star, counts["step"])."""
+    lib = opcount_lib()
+    nv = nvar_of(model)
+    flux = np.zeros(nv)
+    us = C.c_double()
+    zs = C.c_double()
+    raw = np.zeros(len(OP_PHASES) * len(OP_CATEGORIES), dtype=np.uint64)
+    st = np.ascontiguousarray(stencil, dtype=np.float64)
+    lib.opcount_face(MODEL_ID[model], C.byref(p), _dptr(st), dt, dx, _dptr(flux), C.byref(us),
+                     C.byref(zs), raw.ctypes.data_as(C.POINTER(C.c_uint64)))
+    return flux, us.value, (zs.value if model == "allaire" else None), _counts_dict(raw)["step"]
+
+
 def build(quiet: bool = True, ref: bool | None = None) -> None:
     """Build the oracles with oracle/Makefile (the reference part only where
     the reference sources are present)."""
     import subprocess
 
-    targets = ["port"]
+    targets = ["port", "opcount"]
     ref_src = Path(os.environ.get("CFD_REFERENCE_DIR", "/root/reference"))
     if ref is None:
         ref = ref_src.exists()
