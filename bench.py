@@ -218,9 +218,9 @@ def _ref_rate(O, G, recipe, n_x, n_y, nbub, budget_s, cores):
     return n_x * n_y * taken, f(), taken
 
 
-def cpu_baseline(workload: str, budget_s: float = 16.0) -> dict:
+def cpu_baseline(workload: str, budget_s: float = 16.0, single_thread_s: float = 5.0) -> dict:
     """The reference's own CPU code (oracle/_ref, all host threads) on a
-    bounded sample of the workload."""
+    bounded sample of the workload, plus a one-thread run (`single_thread`)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import cfdgpu as G
     import oracle_py as O
@@ -241,8 +241,23 @@ def cpu_baseline(workload: str, budget_s: float = 16.0) -> dict:
         cells += c
         secs += s
         desc.append(f"{recipe} {nx}x{ny} x {k} steps")
-    return {"value": cells / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": "; ".join(desc) + f" ({cores} OpenMP threads, time loop only, {secs:.1f} s)"}
+    out = {"value": cells / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
+           "sample": "; ".join(desc) + f" ({cores} OpenMP threads, time loop only, {secs:.1f} s)"}
+    # The same code on one thread (deterministic: with more threads the
+    # reference's compute_dt races on its maxima), on a smaller sample of the
+    # same recipes so that it stays within a few seconds.
+    cells = secs = 0.0
+    desc = []
+    for recipe, nx, ny, nb, share in parts:
+        sx, sy = (256, 256) if recipe == "shock_bubbles" else (256, 128)
+        c, s, k = _ref_rate(O, G, recipe, sx, sy, nb, single_thread_s * share, 1)
+        cells += c
+        secs += s
+        desc.append(f"{recipe} {sx}x{sy} x {k} steps")
+    out["single_thread"] = {"value": cells / secs / 1e9, "unit": UNIT, "cores": 1,
+                            "sample": "; ".join(desc) + f" (1 thread, time loop only, "
+                                                        f"{secs:.1f} s)"}
+    return out
 
 
 def run_reference(args) -> None:
