@@ -199,6 +199,19 @@ def build_ic(G, recipe, nx, ny, seed, nbub):
 
 # ------------------------------------------------------------ CPU baseline --
 
+def _cpu_model() -> str:
+    """The host CPU's model name (first entry of /proc/cpuinfo)."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
 def _ref_rate(O, G, recipe, n_x, n_y, nbub, budget_s, cores):
     import ctypes
 
@@ -242,6 +255,7 @@ def cpu_baseline(workload: str, budget_s: float = 16.0, single_thread_s: float =
         secs += s
         desc.append(f"{recipe} {nx}x{ny} x {k} steps")
     out = {"value": cells / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
+           "cpu_model": _cpu_model(),
            "sample": "; ".join(desc) + f" ({cores} OpenMP threads, time loop only, {secs:.1f} s)"}
     # The same code on one thread (deterministic: with more threads the
     # reference's compute_dt races on its maxima), on a smaller sample of the
@@ -308,6 +322,7 @@ def run_reference(args) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": w, "sample": sample},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "cpu_model": _cpu_model(),
                          "sample": sample},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
