@@ -1,0 +1,41 @@
+"""The CPU legs of bench.py, which need no GPU: the reference arm's JSON line
+and the cpu_baseline record (all-threads and one-thread runs of the
+reference's own code, oracle/_ref), on tiny budgets."""
+import json
+import subprocess
+import sys
+
+import pytest
+
+import oracle_py as O
+from cfdtest import ROOT
+
+pytestmark = pytest.mark.skipif(not (O.ref_available("euler") and O.ref_available("allaire")),
+                                reason="oracle/_ref (reference build) not built")
+
+
+def test_cpu_baseline_record():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    r = bench.cpu_baseline("allaire2048", budget_s=0.5, single_thread_s=0.3)
+    assert r["kind"] == "reference" and r["unit"] == bench.UNIT
+    assert r["value"] > 0 and r["cores"] >= 1 and r["cpu_model"]
+    assert "water_shock_air_bubble 512x256" in r["sample"]
+    st = r["single_thread"]
+    assert st["cores"] == 1 and st["value"] > 0
+    assert "water_shock_air_bubble 256x128" in st["sample"]
+
+
+def test_reference_arm_line():
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference",
+                          "--workload", "allaire2048", "--steps", "2", "--warmup", "1"],
+                         capture_output=True, text=True, timeout=600, check=True)
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    r = json.loads(lines[0])
+    assert r["impl"] == "reference" and r["steps"] == 2 and r["warmup"] == 1
+    assert r["value"] > 0 and r["higher_is_better"] is True
+    assert r["e2e"]["value"] == r["value"]
+    assert r["e2e"]["h2d_bytes_per_step"] == 0 and r["e2e"]["d2h_bytes_per_step"] == 0
+    assert r["cpu_baseline"]["value"] == r["value"] and r["cpu_baseline"]["cores"] >= 1
