@@ -299,8 +299,9 @@ def opcount_face(model: str, p: RefParams, stencil: np.ndarray, dt: float, dx: f
 
 
 def build(quiet: bool = True, ref: bool | None = None) -> None:
-    """Build the oracles with oracle/Makefile (the reference part only where
-    the reference sources are present)."""
+    """Build the oracles with oracle/Makefile (the reference part, and the
+    reference's main loop linked with the GPU adapter, only where the
+    reference sources are present)."""
     import subprocess
 
     targets = ["port", "opcount"]
@@ -309,5 +310,7 @@ def build(quiet: bool = True, ref: bool | None = None) -> None:
         ref = ref_src.exists()
     if ref:
         targets.append("ref")
+        if (HERE.parent / "cfd-art_b200" / "lib" / "libcfdgpu.so").exists():
+            targets.append("adapter")  # the reference's main loop on the GPU adapter
     subprocess.run(["make", "-C", str(HERE), f"REF={ref_src}", "-j8", *targets], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)

@@ -1,0 +1,69 @@
+"""The reference's own main loop with the GPU problem adapter
+(cfd-art_b200/adapter/gpu_problem.hpp) registered in place of its CPU problem.
+
+oracle/Makefile's `adapter` target compiles the reference's main loop,
+splitting schemes, set_ICs and writers from its sources with the adapter, in
+two links: against the library (ref_main_gpu_*) and against a test-only device
+stub whose device calls the CPU oracle answers (ref_main_stub_*,
+tests/adapter/device_stub.cpp).  The stub build must write every output file
+of the reference's own run byte for byte -- which checks the adapter's call
+sequence (which call takes the step, when the state is read back, where the
+masses go) -- and the library build must fail loudly where no GPU exists.
+"""
+import os
+import subprocess
+
+import pytest
+
+from cfdtest import GOLDEN, ROOT, load_golden
+
+REF = ROOT / "oracle" / "_ref"
+RUNS = sorted(p.stem for p in GOLDEN.glob("outputs_*.npz"))
+
+pytestmark = pytest.mark.skipif(not (REF / "ref_main_stub_euler").exists(),
+                                reason="adapter builds absent (need the reference sources)")
+
+
+def _model(run: str) -> str:
+    return "euler" if run.startswith("outputs_euler") else "allaire"
+
+
+def _run(binary, fx, tmp_path, threads=2):
+    out = tmp_path / "out"
+    out.mkdir()
+    sf = tmp_path / "settingsfile.txt"
+    sf.write_text(str(fx["settings"]).format(out=str(out) + "/"))
+    r = subprocess.run([str(binary), str(sf)], capture_output=True, text=True, timeout=300,
+                       env={**os.environ, "OMP_NUM_THREADS": str(threads)})
+    files = {p.name: p.read_bytes() for p in sorted(out.iterdir())}
+    return r, files
+
+
+@pytest.mark.parametrize("run", RUNS)
+def test_adapter_on_device_stub_writes_reference_outputs(run, tmp_path):
+    fx = load_golden(run)
+    r, files = _run(REF / f"ref_main_stub_{_model(run)}", fx, tmp_path)
+    assert r.returncode == 0, r.stderr
+    expected = {k: bytes(v) for k, v in fx.items() if k != "settings"}
+    assert sorted(files) == sorted(expected)
+    for name, data in expected.items():
+        assert files[name] == data, name
+
+
+def _has_device() -> bool:
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_device(), reason="checks the no-device error path")
+@pytest.mark.parametrize("model", ["euler", "allaire"])
+def test_adapter_on_library_fails_loudly_without_device(model, tmp_path):
+    run = next(r for r in RUNS if _model(r) == model)
+    r, files = _run(REF / f"ref_main_gpu_{model}", load_golden(run), tmp_path)
+    assert r.returncode == 1
+    assert "cfd_create failed (-2)" in r.stderr
+    assert files == {}
