@@ -22,6 +22,7 @@
 
 #include "../../include/cfdgpu.h"
 #include "../../include/cfdgpu_host.h"
+#include "cfd_error.h"
 #include "ic_builders.h"
 
 using cfdic::Op;
@@ -627,7 +628,7 @@ int recipe_program(const cfd_config* cfg, int recipe, uint64_t seed, int nbubble
 extern "C" {
 
 int cfd_ic_grid_elems(const cfd_config* cfg, size_t* elems) {
-    if (!cfg || !elems) return CFD_ERR_INVALID;
+    if (!cfg || !elems) return cfd_fail(CFD_ERR_INVALID, "cfd_ic_grid_elems: null argument");
     int g = cfg->flux_solver == CFD_FLUX_GODUNOV ? 1 : 2;
     *elems = (size_t)cfd_nvar(cfg->model) * (cfg->nx + 2 * g) * (size_t)(cfg->ny + 2 * g);
     return CFD_OK;
@@ -635,12 +636,19 @@ int cfd_ic_grid_elems(const cfd_config* cfg, size_t* elems) {
 
 int cfd_case_config(int model, const char* test_case, int nx, int ny, int flux_solver,
                     cfd_config* cfg) {
-    if (!test_case || !cfg || nx < 2 || ny < 2) return CFD_ERR_INVALID;
+    if (!test_case || !cfg) return cfd_fail(CFD_ERR_INVALID, "cfd_case_config: null argument");
+    if (nx < 2 || ny < 2)
+        return cfd_fail(CFD_ERR_INVALID, "grid %dx%d: need at least 2 cells per direction", nx, ny);
+    if (model != CFD_MODEL_EULER && model != CFD_MODEL_ALLAIRE)
+        return cfd_fail(CFD_ERR_INVALID, "unknown model %d", model);
     base_cfg(cfg, model, nx, ny, flux_solver);
     std::string tc = test_case;
-    if (model == CFD_MODEL_EULER) return euler_params(tc, cfg) ? CFD_OK : CFD_ERR_INVALID;
+    if (model == CFD_MODEL_EULER) {
+        if (euler_params(tc, cfg)) return CFD_OK;
+        return cfd_fail(CFD_ERR_INVALID, "unknown Euler test case '%s'", test_case);
+    }
     const ACase* a = allaire_lookup(tc);
-    if (!a) return CFD_ERR_INVALID;
+    if (!a) return cfd_fail(CFD_ERR_INVALID, "unknown Allaire test case '%s'", test_case);
     cfg->gamma1 = a->g1;
     cfg->gamma2 = a->g2;
     cfg->pinf1 = a->p1;
@@ -655,7 +663,7 @@ int cfd_case_config(int model, const char* test_case, int nx, int ny, int flux_s
 }
 
 int cfd_case_ic(const cfd_config* cfg, const char* test_case, uint64_t seed, double* grid) {
-    if (!cfg || !test_case || !grid) return CFD_ERR_INVALID;
+    if (!cfg || !test_case || !grid) return cfd_fail(CFD_ERR_INVALID, "cfd_case_ic: null argument");
     Grid G = make_grid(cfg, grid);
     memset(grid, 0, sizeof(double) * G.nv * G.rows() * G.cols());
     std::vector<Op> ops;
@@ -665,13 +673,15 @@ int cfd_case_ic(const cfd_config* cfg, const char* test_case, uint64_t seed, dou
         allaire_per_cell_ic(test_case, q, G);
         return CFD_OK;
     }
-    if (r) return r;
+    if (r) return cfd_fail(r, "unknown test case '%s' for model %d", test_case, cfg->model);
     run_program(G, ops, q);
     return CFD_OK;
 }
 
 int cfd_recipe_config(int recipe, int nx, int ny, cfd_config* cfg) {
-    if (!cfg || nx < 2 || ny < 2) return CFD_ERR_INVALID;
+    if (!cfg) return cfd_fail(CFD_ERR_INVALID, "cfd_recipe_config: null argument");
+    if (nx < 2 || ny < 2)
+        return cfd_fail(CFD_ERR_INVALID, "grid %dx%d: need at least 2 cells per direction", nx, ny);
     switch (recipe) {
         case CFD_RECIPE_FOUR_QUADRANT:
             base_cfg(cfg, CFD_MODEL_EULER, nx, ny, CFD_FLUX_MUSCL);
@@ -707,16 +717,17 @@ int cfd_recipe_config(int recipe, int nx, int ny, cfd_config* cfg) {
             set_bcs(cfg, TR, TR, TR, TR);
             return CFD_OK;
     }
-    return CFD_ERR_INVALID;
+    return cfd_fail(CFD_ERR_INVALID, "unknown recipe %d", recipe);
 }
 
 int cfd_recipe_ic(const cfd_config* cfg, int recipe, uint64_t seed, int nbubbles, double* grid) {
-    if (!cfg || !grid) return CFD_ERR_INVALID;
+    if (!cfg || !grid) return cfd_fail(CFD_ERR_INVALID, "cfd_recipe_ic: null argument");
     Grid G = make_grid(cfg, grid);
     std::vector<Op> ops;
     cfdic::Eos q;
     int r = cfdic::recipe_program(cfg, recipe, seed, nbubbles, ops, q);
-    if (r) return r;
+    if (r) return cfd_fail(r, "recipe %d does not apply to this configuration (model %d)", recipe,
+                           cfg->model);
     run_program(G, ops, q);
     return CFD_OK;
 }

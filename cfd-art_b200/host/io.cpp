@@ -10,6 +10,7 @@
 #include "../../include/cfdgpu.h"
 #include "../../include/cfdgpu_host.h"
 #include "cfd_checkpoint.h"
+#include "cfd_error.h"
 
 namespace {
 
@@ -54,11 +55,29 @@ double mixture_pressure(const cfd_config* c, double rho, double e, double z) {
     return rho * e / eps - k;
 }
 
+// Values of the optional settings keys; -1 for a value the key does not take.
 int lim_of(const std::string& s) {
+    if (s == "minmod") return CFD_LIM_MINMOD;
     if (s == "vanleer" || s == "van_leer") return CFD_LIM_VANLEER;
     if (s == "mc" || s == "MC") return CFD_LIM_MC;
     if (s == "unlimited") return CFD_LIM_UNLIMITED;
-    return CFD_LIM_MINMOD;
+    return -1;
+}
+
+int wavespeed_of(const std::string& s) {
+    if (s == "davis") return CFD_WS_DAVIS;
+    if (s == "pvrs") return CFD_WS_PVRS;
+    return -1;
+}
+
+int precision_of(const std::string& s) {
+    if (s == "fp64") return CFD_PREC_FP64;
+    if (s == "mixed") return CFD_PREC_MIXED;
+    return -1;
+}
+
+int cannot_write(const std::string& name) {
+    return cfd_fail(CFD_ERR_INVALID, "cannot open output file '%s'", name.c_str());
 }
 
 int recipe_of(const std::string& tc) {
@@ -74,12 +93,12 @@ extern "C" {
 
 // headers/settings_file.hpp:35-71
 int cfd_read_settings(const char* path, cfd_settings* s) {
-    if (!path || !s) return CFD_ERR_INVALID;
+    if (!path || !s) return cfd_fail(CFD_ERR_INVALID, "cfd_read_settings: null argument");
     memset(s, 0, sizeof *s);
     s->seed = 20261203ULL;
     s->nbubbles = 32;
     std::ifstream in(path);
-    if (!in) return CFD_ERR_INVALID;
+    if (!in) return cfd_fail(CFD_ERR_INVALID, "cannot open settings file '%s'", path);
     std::string line;
     while (std::getline(in, line)) {
         std::istringstream iss(line);
@@ -114,33 +133,61 @@ int cfd_read_settings(const char* path, cfd_settings* s) {
 }
 
 int cfd_settings_config(const cfd_settings* s, cfd_config* cfg) {
-    if (!s || !cfg) return CFD_ERR_INVALID;
+    if (!s || !cfg) return cfd_fail(CFD_ERR_INVALID, "cfd_settings_config: null argument");
     std::string prob = s->problem;
     int model = (prob == "allaire" || prob == "allaire_diffuse") ? CFD_MODEL_ALLAIRE
                                                                  : CFD_MODEL_EULER;
-    if (prob != "euler" && model == CFD_MODEL_EULER) return CFD_ERR_INVALID;
+    if (prob != "euler" && model == CFD_MODEL_EULER)
+        return cfd_fail(CFD_ERR_INVALID, "settings: unknown problem '%s' (euler, allaire)",
+                        s->problem);
     std::string fs = s->flux_solver;
     int flux;
     if (fs == "MUSCL") flux = CFD_FLUX_MUSCL;
     else if (fs == "Godunov") flux = CFD_FLUX_GODUNOV;
-    else return CFD_ERR_INVALID;
-    if (std::string(s->riemann_solver) != "HLLC") return CFD_ERR_INVALID;
+    else
+        return cfd_fail(CFD_ERR_INVALID, "settings: unknown flux_solver '%s' (MUSCL, Godunov)",
+                        s->flux_solver);
+    if (std::string(s->riemann_solver) != "HLLC")
+        return cfd_fail(CFD_ERR_INVALID, "settings: unknown riemann_solver '%s' (HLLC)",
+                        s->riemann_solver);
+    std::string sp = s->splitting_scheme;
+    int split;
+    if (sp == "naive_splitting") split = CFD_SPLIT_NAIVE;
+    else if (sp == "strang_splitting") split = CFD_SPLIT_STRANG;
+    else
+        return cfd_fail(CFD_ERR_INVALID,
+                        "settings: unknown splitting_scheme '%s' (naive_splitting, "
+                        "strang_splitting)",
+                        s->splitting_scheme);
+    int lim = s->limiter[0] ? lim_of(s->limiter) : 0;
+    if (lim < 0)
+        return cfd_fail(CFD_ERR_INVALID,
+                        "settings: unknown limiter '%s' (minmod, vanleer, mc, unlimited)",
+                        s->limiter);
+    int ws = s->wavespeed[0] ? wavespeed_of(s->wavespeed) : 0;
+    if (ws < 0)
+        return cfd_fail(CFD_ERR_INVALID, "settings: unknown wavespeed '%s' (davis, pvrs)",
+                        s->wavespeed);
+    int prec = s->precision[0] ? precision_of(s->precision) : CFD_PREC_FP64;
+    if (prec < 0)
+        return cfd_fail(CFD_ERR_INVALID, "settings: unknown precision '%s' (fp64, mixed)",
+                        s->precision);
     int r;
     int rec = recipe_of(s->test_case);
     if (rec) r = cfd_recipe_config(rec, s->Nx, s->Ny, cfg);
     else r = cfd_case_config(model, s->test_case, s->Nx, s->Ny, flux, cfg);
-    if (r) return r;
+    if (r) return r;  // with its message
+    if (rec && cfg->model != model)
+        return cfd_fail(CFD_ERR_INVALID, "settings: test_case '%s' is not a %s problem",
+                        s->test_case, s->problem);
     cfg->flux_solver = flux;
     cfg->cfl = s->CFL;
-    std::string sp = s->splitting_scheme;
-    if (sp == "naive_splitting") cfg->splitting = CFD_SPLIT_NAIVE;
-    else if (sp == "strang_splitting") cfg->splitting = CFD_SPLIT_STRANG;
-    else return CFD_ERR_INVALID;
-    if (s->limiter[0]) cfg->limiter = lim_of(s->limiter);
-    if (s->wavespeed[0]) cfg->wavespeed = std::string(s->wavespeed) == "pvrs" ? CFD_WS_PVRS : CFD_WS_DAVIS;
+    cfg->splitting = split;
+    if (s->limiter[0]) cfg->limiter = lim;
+    if (s->wavespeed[0]) cfg->wavespeed = ws;
     if (s->alpha_clip > 0.0) cfg->z_min = s->alpha_clip;
     cfg->fix_dy_halfstep = s->fix_dy_halfstep;
-    cfg->precision = std::string(s->precision) == "mixed" ? CFD_PREC_MIXED : CFD_PREC_FP64;
+    cfg->precision = prec;
     return CFD_OK;
 }
 
@@ -152,10 +199,11 @@ int cfd_settings_ic(const cfd_settings* s, const cfd_config* cfg, double* grid) 
 
 // E/sourcecode/euler_io.cpp:1188-1216, A/sourcecode/allaire_diffuse_io.cpp:1153-1186
 int cfd_write_state(const cfd_config* c, const double* grid, const char* basename, double t) {
-    if (!c || !grid || !basename) return CFD_ERR_INVALID;
+    if (!c || !grid || !basename) return cfd_fail(CFD_ERR_INVALID, "cfd_write_state: null argument");
     View v = view_of(c, grid);
-    std::ofstream out(std::string(basename) + "-state-" + std::to_string(t) + ".dat");
-    if (!out) return CFD_ERR_INVALID;
+    const std::string name = std::string(basename) + "-state-" + std::to_string(t) + ".dat";
+    std::ofstream out(name);
+    if (!out) return cannot_write(name);
     for (int i = v.g; i < v.ny + v.g; ++i) {
         for (int j = v.g; j < v.nx + v.g; ++j) {
             const double* U = v.cell(i, j);
@@ -189,7 +237,8 @@ int cfd_write_state(const cfd_config* c, const double* grid, const char* basenam
 
 // E/sourcecode/euler_io.cpp:1142-1185 (A: :1109-1150): |grad rho| / max.
 int cfd_write_schlieren(const cfd_config* c, const double* grid, const char* basename, double t) {
-    if (!c || !grid || !basename) return CFD_ERR_INVALID;
+    if (!c || !grid || !basename)
+        return cfd_fail(CFD_ERR_INVALID, "cfd_write_schlieren: null argument");
     View v = view_of(c, grid);
     std::vector<double> g;
     g.reserve((size_t)v.nx * v.ny);
@@ -206,11 +255,13 @@ int cfd_write_schlieren(const cfd_config* c, const double* grid, const char* bas
 
 int cfd_write_schlieren_field(const cfd_config* c, const double* field, const char* basename,
                               double t) {
-    if (!c || !field || !basename) return CFD_ERR_INVALID;
+    if (!c || !field || !basename)
+        return cfd_fail(CFD_ERR_INVALID, "cfd_write_schlieren_field: null argument");
     const size_t n = (size_t)c->nx * c->ny;
     double mx = *std::max_element(field, field + n);
-    std::ofstream out(std::string(basename) + "-schlieren-" + std::to_string(t) + ".dat");
-    if (!out) return CFD_ERR_INVALID;
+    const std::string name = std::string(basename) + "-schlieren-" + std::to_string(t) + ".dat";
+    std::ofstream out(name);
+    if (!out) return cannot_write(name);
     size_t k = 0;
     for (int i = 0; i < c->ny; ++i) {
         const double y = c->y0 + double(i) * c->dy + 0.5 * c->dy;  // cell centres as View
@@ -228,7 +279,9 @@ int cfd_write_schlieren_field(const cfd_config* c, const double* field, const ch
 // of the ghosted grid (ghost cells included), -lineoutx-<n>.dat and
 // -lineouty-<n>.dat.
 int cfd_write_lineout(const cfd_config* c, const double* grid, const char* basename, int n) {
-    if (!c || !grid || !basename || c->model != CFD_MODEL_ALLAIRE) return CFD_ERR_INVALID;
+    if (!c || !grid || !basename) return cfd_fail(CFD_ERR_INVALID, "cfd_write_lineout: null argument");
+    if (c->model != CFD_MODEL_ALLAIRE)
+        return cfd_fail(CFD_ERR_INVALID, "cfd_write_lineout: Allaire grids only");
     View v = view_of(c, grid);
     auto line = [&](std::ofstream& out, double coord, const double* U) {
         double rho = U[0] + U[1];
@@ -240,22 +293,24 @@ int cfd_write_lineout(const cfd_config* c, const double* grid, const char* basen
         out << coord << " " << rho << " " << u << " " << vv << " " << e << " " << p << " " << z
             << std::endl;
     };
-    std::ofstream ox(std::string(basename) + "-lineoutx-" + std::to_string(n) + ".dat");
-    if (!ox) return CFD_ERR_INVALID;
+    const std::string xname = std::string(basename) + "-lineoutx-" + std::to_string(n) + ".dat";
+    std::ofstream ox(xname);
+    if (!ox) return cannot_write(xname);
     int i = v.ny / 2;
     for (int j = 0; j < v.nx + 2 * v.g; ++j) line(ox, v.ccx(j), v.cell(i, j));
     ox.close();
-    std::ofstream oy(std::string(basename) + "-lineouty-" + std::to_string(n) + ".dat");
-    if (!oy) return CFD_ERR_INVALID;
+    const std::string yname = std::string(basename) + "-lineouty-" + std::to_string(n) + ".dat";
+    std::ofstream oy(yname);
+    if (!oy) return cannot_write(yname);
     int j = v.nx / 2;
     for (int r = 0; r < v.ny + 2 * v.g; ++r) line(oy, v.ccy(r), v.cell(r, j));
     return CFD_OK;
 }
 
 int cfd_checkpoint_info(const char* path, cfd_config* cfg, int* n, double* t) {
-    if (!path) return CFD_ERR_INVALID;
+    if (!path) return cfd_fail(CFD_ERR_INVALID, "cfd_checkpoint_info: null path");
     FILE* f = fopen(path, "rb");
-    if (!f) return CFD_ERR_INVALID;
+    if (!f) return cfd_fail(CFD_ERR_INVALID, "cannot open checkpoint '%s'", path);
     cfd::CkptHeader h;
     int r = cfd::ckpt_read_header(f, h);
     fclose(f);
@@ -268,9 +323,13 @@ int cfd_checkpoint_info(const char* path, cfd_config* cfg, int* n, double* t) {
 
 int cfd_write_masschange(const cfd_config* c, const char* basename, int nrec, const double* t,
                          const double* m1, const double* m2) {
-    if (!c || !basename || nrec < 1 || !t || !m1) return CFD_ERR_INVALID;
-    std::ofstream out(std::string(basename) + "-masschange.dat");
-    if (!out) return CFD_ERR_INVALID;
+    if (!c || !basename || nrec < 1 || !t || !m1)
+        return cfd_fail(CFD_ERR_INVALID, "cfd_write_masschange: null argument or no records");
+    if (c->model == CFD_MODEL_ALLAIRE && !m2)
+        return cfd_fail(CFD_ERR_INVALID, "cfd_write_masschange: Allaire needs both mass series");
+    const std::string name = std::string(basename) + "-masschange.dat";
+    std::ofstream out(name);
+    if (!out) return cannot_write(name);
     for (int k = 0; k < nrec; ++k) {
         if (c->model == CFD_MODEL_EULER)
             out << t[k] << " " << m1[k] - m1[0] << std::endl;

@@ -204,3 +204,63 @@ def test_checkpoint_info_rejects_non_checkpoints(tmp_path):
         G.checkpoint_info(f)
     with pytest.raises(G.CfdError):
         G.checkpoint_info(tmp_path / "missing.ckpt")
+
+
+_GOOD_SETTINGS = {"Nx": "30", "Ny": "20", "CFL": "0.5", "splitting_scheme": "naive_splitting",
+                  "test_case": "cross", "output_freq": "3", "outputpath": "./o/",
+                  "flux_solver": "MUSCL", "riemann_solver": "HLLC", "problem": "euler"}
+
+
+@pytest.mark.parametrize("change,message", [
+    ({"problem": "navier"}, "unknown problem 'navier'"),
+    ({"flux_solver": "WENO"}, "unknown flux_solver 'WENO'"),
+    ({"riemann_solver": None}, "unknown riemann_solver ''"),
+    ({"splitting_scheme": "lie"}, "unknown splitting_scheme 'lie'"),
+    ({"test_case": "nonesuch"}, "unknown Euler test case 'nonesuch'"),
+    ({"problem": "allaire", "test_case": "cross"}, "unknown Allaire test case 'cross'"),
+    ({"test_case": "water_shock_air_bubble"}, "is not a euler problem"),
+    ({"Nx": None}, "need at least 2 cells"),
+    ({"Ny": "-4"}, "need at least 2 cells"),
+    ({"Nx": "abc"}, "need at least 2 cells"),
+    ({"limiter": "superbee"}, "unknown limiter 'superbee'"),
+    ({"wavespeed": "roe"}, "unknown wavespeed 'roe'"),
+    ({"precision": "fp16"}, "unknown precision 'fp16'"),
+])
+def test_corrupted_settings_rejected_with_a_message(tmp_path, change, message):
+    """A settings file the reference would assert on (or one with a bad
+    value of an added key) fails with CFD_ERR_INVALID and says why; the
+    reference's parser itself ignores unknown keys, and so does ours."""
+    kv = {**_GOOD_SETTINGS, **change}
+    f = tmp_path / "settingsfile.txt"
+    f.write_text("".join(f"{k} {v}\n" for k, v in kv.items() if v is not None))
+    L = G.lib()
+    st = G.Settings()
+    assert L.cfd_read_settings(str(f).encode(), C.byref(st)) == 0
+    L.cfd_version()  # a successful call leaves the previous message alone
+    cfg = G.Config()
+    assert L.cfd_settings_config(C.byref(st), C.byref(cfg)) == -1
+    assert message in G.last_error()
+
+
+def test_host_hook_errors_carry_messages(tmp_path):
+    L = G.lib()
+    st = G.Settings()
+    assert L.cfd_read_settings(str(tmp_path / "absent.txt").encode(), C.byref(st)) == -1
+    assert "cannot open settings file" in G.last_error()
+    cfg = G.Config()
+    assert L.cfd_case_config(G.EULER, b"nonesuch", 8, 8, 0, C.byref(cfg)) == -1
+    assert "unknown Euler test case 'nonesuch'" in G.last_error()
+    assert L.cfd_recipe_config(99, 8, 8, C.byref(cfg)) == -1
+    assert "unknown recipe 99" in G.last_error()
+    cfg = G.recipe_config("four_quadrant", 8, 8)
+    grid = np.zeros(cfg.ghosted_shape())
+    gp = grid.ctypes.data_as(C.POINTER(C.c_double))
+    assert L.cfd_recipe_ic(C.byref(cfg), 3, C.c_uint64(1), 1, gp) == -1
+    assert "does not apply to this configuration" in G.last_error()
+    base = str(tmp_path / "no_such_dir" / "run").encode()
+    assert L.cfd_write_state(C.byref(cfg), gp, base, C.c_double(0.0)) == -1
+    assert "cannot open output file" in G.last_error()
+    assert L.cfd_write_lineout(C.byref(cfg), gp, base, 0) == -1
+    assert "Allaire grids only" in G.last_error()
+    assert L.cfd_checkpoint_info(str(tmp_path / "absent.ckpt").encode(), None, None, None) == -1
+    assert "cannot open checkpoint" in G.last_error()
