@@ -133,7 +133,9 @@ int validate(const cfd_config* c) {
     if (c->precision != CFD_PREC_FP64 && c->precision != CFD_PREC_MIXED)
         return fail(CFD_ERR_INVALID, "unknown precision %d", c->precision);
     if (c->precision == CFD_PREC_MIXED)
-        return fail(CFD_ERR_UNSUPPORTED, "mixed precision is served by cfd_mixed_* entry points");
+        return fail(CFD_ERR_UNSUPPORTED,
+                    "a single solver is FP64; mixed precision runs as a batch member "
+                    "(cfd_batch_add) or through the server");
     if (c->nx < 2 || c->ny < 2)
         return fail(CFD_ERR_INVALID, "grid %dx%d: need at least 2 cells per direction", c->nx,
                     c->ny);
