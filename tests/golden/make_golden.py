@@ -2,6 +2,7 @@
 
     python tests/golden/make_golden.py            # everything
     python tests/golden/make_golden.py outputs    # only the whole-run output files
+    python tests/golden/make_golden.py adapter    # only the adapter's extra runs (golden/adapter/)
 
 Requires oracle/_ref/libref_{euler,allaire}.so (built by `make -C oracle ref`
 from the reference sources) and cfd-art_b200/lib/libcfdgpu.so (only for the
@@ -156,7 +157,24 @@ OUTPUT_RUNS = [
 ]
 
 
-def output_run(name: str, model: str, settings: str) -> None:
+# More whole runs, for the reference-loop adapter's CPU check only (kept in
+# golden/adapter/ so that the GPU driver test does not collect them): the
+# Godunov scheme (one ghost layer), Strang splitting for Euler, naive
+# splitting for Allaire.
+ADAPTER_RUNS = [
+    ("godunov_totem_pole_2_20x20", "euler",
+     "Nx 20\nNy 20\nCFL 0.5\nsplitting_scheme naive_splitting\ntest_case totem_pole_2\n"
+     "output_freq 2\noutputpath {out}\nflux_solver Godunov\nriemann_solver HLLC\nproblem euler\n"),
+    ("strang_circular_explosion_24x20", "euler",
+     "Nx 24\nNy 20\nCFL 0.5\nsplitting_scheme strang_splitting\ntest_case circular_explosion\n"
+     "output_freq 2\noutputpath {out}\nflux_solver MUSCL\nriemann_solver HLLC\nproblem euler\n"),
+    ("naive_ST2_x_40x6", "allaire",
+     "Nx 40\nNy 6\nCFL 0.5\nsplitting_scheme naive_splitting\ntest_case ST2_x\n"
+     "output_freq 2\noutputpath {out}\nflux_solver MUSCL\nriemann_solver HLLC\nproblem allaire\n"),
+]
+
+
+def output_run(name: str, model: str, settings: str, dest: Path = HERE) -> None:
     import os
     import subprocess
     import tempfile
@@ -172,7 +190,8 @@ def output_run(name: str, model: str, settings: str) -> None:
                        env={**os.environ, "OMP_NUM_THREADS": "1"})
         files = {fn: np.frombuffer(open(os.path.join(out, fn), "rb").read(), np.uint8)
                  for fn in sorted(os.listdir(out))}
-    np.savez_compressed(HERE / f"{name}.npz", settings=np.array(settings), **files)
+    dest.mkdir(exist_ok=True)
+    np.savez_compressed(dest / f"{name}.npz", settings=np.array(settings), **files)
     print(f"{name}: {len(files)} files")
 
 
@@ -180,5 +199,10 @@ if __name__ == "__main__":
     if sys.argv[1:] == ["outputs"]:
         for run in OUTPUT_RUNS:
             output_run(*run)
+    elif sys.argv[1:] == ["adapter"]:
+        for run in ADAPTER_RUNS:
+            output_run(*run, dest=HERE / "adapter")
     else:
         main()
+        for run in ADAPTER_RUNS:
+            output_run(*run, dest=HERE / "adapter")

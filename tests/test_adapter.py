@@ -18,13 +18,19 @@ import pytest
 from cfdtest import GOLDEN, ROOT, load_golden
 
 REF = ROOT / "oracle" / "_ref"
-RUNS = sorted(p.stem for p in GOLDEN.glob("outputs_*.npz"))
+RUNS = sorted(p.stem for p in GOLDEN.glob("outputs_*.npz")) + \
+    sorted("adapter/" + p.stem for p in (GOLDEN / "adapter").glob("*.npz"))
+MODELS = {"adapter/godunov_totem_pole_2_20x20": "euler",
+          "adapter/strang_circular_explosion_24x20": "euler",
+          "adapter/naive_ST2_x_40x6": "allaire"}
 
 pytestmark = pytest.mark.skipif(not (REF / "ref_main_stub_euler").exists(),
                                 reason="adapter builds absent (need the reference sources)")
 
 
 def _model(run: str) -> str:
+    if run in MODELS:
+        return MODELS[run]
     return "euler" if run.startswith("outputs_euler") else "allaire"
 
 
