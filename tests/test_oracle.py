@@ -61,6 +61,12 @@ LIVE = [
     ("allaire", "shocked_helium_bubble", 40, 20, 20, {}),
     ("allaire", "ST2_x", 60, 10, 40, {"wavespeed": 1, "z_min": 1e-6}),
     ("allaire", "ST1_x", 40, 6, 20, {"flux_solver": 1}),
+    ("allaire", "shocked_helium_bubble", 30, 12, 20, {"splitting": 1}),
+    ("allaire", "ST2_y", 8, 40, 30, {"fix_dy_halfstep": 1, "limiter": 1}),
+    ("allaire", "TTC3_x_pure", 40, 6, 30, {"flux_solver": 1, "splitting": 1}),
+    ("allaire", "ST2_x", 40, 8, 30, {"bc": (1, 0, 1, 1), "wavespeed": 1}),
+    ("euler", "totem_pole_2", 20, 24, 30, {"flux_solver": 1, "splitting": 1}),
+    ("euler", "cross", 24, 20, 30, {"bc": (1, 1, 1, 1)}),
 ]
 
 
@@ -71,7 +77,10 @@ def test_port_matches_reference_build(model, case, nx, ny, steps, over):
     grid, p = O.ref_case_ic(model, case, nx, ny, fs)
     p.cfl = over.get("cfl", 0.5)
     for k, v in over.items():
-        if k != "cfl":
+        if k == "bc":  # reflective walls where the test case has none
+            for side in range(4):
+                p.bc[side] = v[side]
+        elif k != "cfl":
             setattr(p, k, v)
     g2 = grid.copy()
     a = O.ref_run(model, p, grid, steps)
