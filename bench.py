@@ -19,9 +19,9 @@ free HBM.  K = --steps requests are timed after W = --warmup requests.
              in host memory; cell-updates of all requests / makespan.  p50/p99
              completion latency come from this run.
   plain_fp64 the same served run in the plain FP64 form (bit-identical to the
-             reference), for the "mixed vs plain" comparison; l1_vs_fp64 is
-             the largest relative L1 density error of a mixed result against
-             its FP64 result.
+             reference), for the "mixed vs plain" comparison; l1_vs_fp64 and
+             linf_vs_fp64 are the largest (and median) relative L1 and L-inf
+             density errors of a mixed result against its FP64 result.
   roofline   the dominant mixed sweep kernel on a resident sample of the
              requests: algorithmic bytes (cells x nvar x (4+4) B read + write)
              over its mean CUDA-event launch time, against MEASURED_PEAKS.json.
@@ -153,10 +153,19 @@ def _gpu_id(torch, dev: int) -> str | None:
         return None
 
 
+def _interior_density(a: np.ndarray, model: int) -> np.ndarray:
+    return a[2:-2, 2:-2, 0] if model == 0 else a[2:-2, 2:-2, 0] + a[2:-2, 2:-2, 1]
+
+
 def _rel_l1_density(a: np.ndarray, b: np.ndarray, model: int) -> float:
-    ra = a[2:-2, 2:-2, 0] if model == 0 else a[2:-2, 2:-2, 0] + a[2:-2, 2:-2, 1]
-    rb = b[2:-2, 2:-2, 0] if model == 0 else b[2:-2, 2:-2, 0] + b[2:-2, 2:-2, 1]
+    ra, rb = _interior_density(a, model), _interior_density(b, model)
     return float(np.abs(ra - rb).sum() / np.abs(rb).sum())
+
+
+def _rel_linf_density(a: np.ndarray, b: np.ndarray, model: int) -> float:
+    """max |rho_a - rho_b| / max |rho_b| over the interior cells."""
+    ra, rb = _interior_density(a, model), _interior_density(b, model)
+    return float(np.abs(ra - rb).max() / np.abs(rb).max())
 
 
 # ------------------------------------------------------- request streams --
@@ -628,6 +637,8 @@ def bench_served(args, ctx, G, stream, clocks):
     lat_f = [i.latency_s for i, _ in res_f]
     pct = lambda v, q: float(np.percentile(v, q))
     l1 = [_rel_l1_density(a, f, c.model) for (_, a), (_, f), (c, _) in zip(res_m, res_f, timed_ics)]
+    linf = [_rel_linf_density(a, f, c.model)
+            for (_, a), (_, f), (c, _) in zip(res_m, res_f, timed_ics)]
     nbytes = sum(ic.size * 8 for _, ic in timed_ics)
     e2e_val = ctx.sum(upd) / ctx.max(mk_m) / 1e9
     fp64_val = ctx.sum(upd) / ctx.max(mk_f) / 1e9
@@ -650,6 +661,7 @@ def bench_served(args, ctx, G, stream, clocks):
                        "device_s": st_f.device_s, "max_resident": st_f.max_running},
         "mixed_vs_plain": e2e_val / fp64_val,
         "l1_vs_fp64": {"max": max(l1), "median": float(np.median(l1)), "bound": 1e-4},
+        "linf_vs_fp64": {"max": max(linf), "median": float(np.median(linf))},
         "clocks": ck, "gpu_launches": 2 * models * max_steps,
         "roofline": rl,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes / len(timed),

@@ -1,6 +1,7 @@
-"""The CPU legs of bench.py, which need no GPU: the reference arm's JSON line
-and the cpu_baseline record (all-threads and one-thread runs of the
-reference's own code, oracle/_ref), on tiny budgets."""
+"""The CPU legs of bench.py, which need no GPU: the reference arm's JSON line,
+the cpu_baseline record (all-threads and one-thread runs of the reference's
+own code, oracle/_ref) on tiny budgets, and the density error measures the
+served line reports."""
 import json
 import subprocess
 import sys
@@ -39,3 +40,22 @@ def test_reference_arm_line():
     assert r["e2e"]["value"] == r["value"]
     assert r["e2e"]["h2d_bytes_per_step"] == 0 and r["e2e"]["d2h_bytes_per_step"] == 0
     assert r["cpu_baseline"]["value"] == r["value"] and r["cpu_baseline"]["cores"] >= 1
+
+
+def test_density_error_measures():
+    sys.path.insert(0, str(ROOT))
+    import numpy as np
+
+    import bench
+
+    rng = np.random.default_rng(3)
+    for model, nv in ((0, 4), (1, 6)):
+        ref = rng.uniform(0.5, 2.0, size=(12, 10, nv))
+        got = ref.copy()
+        assert bench._rel_l1_density(got, ref, model) == 0.0
+        assert bench._rel_linf_density(got, ref, model) == 0.0
+        got[5, 4, 0] += 1e-3  # one interior cell; ghost cells (first/last two) never count
+        got[0, 0, 0] += 1.0
+        rho = ref[2:-2, 2:-2, 0] if model == 0 else ref[2:-2, 2:-2, 0] + ref[2:-2, 2:-2, 1]
+        assert np.isclose(bench._rel_l1_density(got, ref, model), 1e-3 / np.abs(rho).sum())
+        assert np.isclose(bench._rel_linf_density(got, ref, model), 1e-3 / np.abs(rho).max())
