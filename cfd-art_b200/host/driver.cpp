@@ -115,6 +115,17 @@ int main(int argc, char** argv) {
     cfd_get_status(s, &st);
     std::printf("[simulation] %d steps, t = %g\n", n, t);
     std::printf("[main] The wall clock runtime was %gs.\n", secs);
+    // One machine-readable line: the run's size, time and the device's event counters
+    // (wall time includes the initial upload and every output written).
+    const double updates = (double)cfg.nx * cfg.ny * n;
+    std::printf("[metrics] {\"model\": \"%s\", \"nx\": %d, \"ny\": %d, \"steps\": %d, \"t\": %.17g, "
+                "\"cell_updates\": %.17g, \"wall_s\": %.6f, \"gcell_updates_per_s\": %.6g, "
+                "\"counters\": {\"unphysical_input\": %llu, \"slope_zeroed\": %llu, "
+                "\"first_order\": %llu, \"fixup\": %llu, \"unphysical_output\": %llu}}\n",
+                allaire ? "allaire" : "euler", cfg.nx, cfg.ny, n, t, updates, secs,
+                secs > 0.0 ? updates / secs / 1e9 : 0.0, st.counters[CFD_CNT_UNPHYSICAL_INPUT],
+                st.counters[CFD_CNT_SLOPE_ZEROED], st.counters[CFD_CNT_FIRST_ORDER],
+                st.counters[CFD_CNT_FIXUP], st.counters[CFD_CNT_UNPHYSICAL_OUTPUT]);
     if (st.counters[CFD_CNT_UNPHYSICAL_INPUT] || st.counters[CFD_CNT_UNPHYSICAL_OUTPUT])
         std::printf("[main] warning: %llu unphysical states reached the flux solver\n",
                     st.counters[CFD_CNT_UNPHYSICAL_INPUT] + st.counters[CFD_CNT_UNPHYSICAL_OUTPUT]);
