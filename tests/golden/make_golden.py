@@ -171,6 +171,9 @@ ADAPTER_RUNS = [
     ("naive_ST2_x_40x6", "allaire",
      "Nx 40\nNy 6\nCFL 0.5\nsplitting_scheme naive_splitting\ntest_case ST2_x\n"
      "output_freq 2\noutputpath {out}\nflux_solver MUSCL\nriemann_solver HLLC\nproblem allaire\n"),
+    ("godunov_ST1_x_30x6", "allaire",
+     "Nx 30\nNy 6\nCFL 0.5\nsplitting_scheme strang_splitting\ntest_case ST1_x\n"
+     "output_freq 2\noutputpath {out}\nflux_solver Godunov\nriemann_solver HLLC\nproblem allaire\n"),
 ]
 
 

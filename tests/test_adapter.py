@@ -22,7 +22,8 @@ RUNS = sorted(p.stem for p in GOLDEN.glob("outputs_*.npz")) + \
     sorted("adapter/" + p.stem for p in (GOLDEN / "adapter").glob("*.npz"))
 MODELS = {"adapter/godunov_totem_pole_2_20x20": "euler",
           "adapter/strang_circular_explosion_24x20": "euler",
-          "adapter/naive_ST2_x_40x6": "allaire"}
+          "adapter/naive_ST2_x_40x6": "allaire",
+          "adapter/godunov_ST1_x_30x6": "allaire"}
 
 pytestmark = pytest.mark.skipif(not (REF / "ref_main_stub_euler").exists(),
                                 reason="adapter builds absent (need the reference sources)")
