@@ -312,6 +312,16 @@ void worker_main(cfd_server* s) {
                                                        0, 0.0)
                                    : cfd_upload(r->solver, r->grid, CFD_LAYOUT_GHOSTED_AOS,
                                                 0, 0.0);
+                if (rc) {
+                    // a failed start gives back everything it took: finish() returns
+                    // the request's bytes to the budget, so its device state must go too
+                    if (r->solver) cfd_destroy(r->solver);
+                    r->solver = nullptr;
+                    if (r->stream) cudaStreamDestroy(r->stream);
+                    r->stream = nullptr;
+                    if (r->ev) cudaEventDestroy(r->ev);
+                    r->ev = nullptr;
+                }
             }
             std::lock_guard<std::mutex> lk(s->mu);
             if (rc) {
