@@ -3,7 +3,7 @@
 //
 // The reference drives a problem through simulation::run_simulation
 // (headers/simulation.hpp:36-67) and the splitting scheme named in the
-// settings file (headers/splitting_scheme.hpp:29-137).  Registered in place
+// settings file (headers/splitting_scheme.hpp:29-143).  Registered in place
 // of the CPU problem, this class keeps that loop, the settings file, the
 // reference's set_ICs and its output writers, and moves the state and the
 // time step to the GPU:
