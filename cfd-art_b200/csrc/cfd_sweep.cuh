@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(256, MODEL == MODEL_EULER ? 3 : 2) sweep_kerne
         if constexpr (MODEL == MODEL_ALLAIRE) {
             double cs = copysign(1.0, us);
             double zs;
-            if (A.godunov)  // A/headers/flux_solver_godunov.hpp:32-33
+            if (A.godunov)  // A/headers/flux_solver_godunov.hpp:33-34
                 zs = (((1.0 + cs) / 2.0) * EL[5]) + (((1.0 - cs) / 2.0) * ER[5]);
             else  // A/headers/flux_solver_MUSCLhancock.hpp:375
                 zs = ((0.5 * (1.0 + cs)) * EL[5]) + ((0.5 * (1.0 - cs)) * ER[5]);
@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(256, MODEL == MODEL_EULER ? 3 : 2) sweep_kerne
             snap_allaire(N, changed);  // live assert(is_physical_state(...))
             ev_bad |= !is_physical_exact<MODEL>(N);
         }
-        if (DIR == DIR_Y) {  // rotate back (E/sourcecode/euler_colsweep.cpp:163-168)
+        if (DIR == DIR_Y) {  // rotate back (E/sourcecode/euler_colsweep.cpp:66-73)
             double t = N[MT::IM];
             N[MT::IM] = -N[MT::IT];
             N[MT::IT] = t;

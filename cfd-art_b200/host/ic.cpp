@@ -366,7 +366,7 @@ bool allaire_per_cell_case(const std::string& tc) {
     return tc == "shocked_SF6" || tc == "TSTM" || tc == "RMI_SF6" || tc == "tin_air_implosion";
 }
 
-// A/sourcecode/allaire_diffuse_io.cpp:401-640 (initial states built from
+// A/sourcecode/allaire_diffuse_io.cpp:402-640 (initial states built from
 // the shape helpers)
 bool allaire_case_program(const std::string& tc, Prog& P) {
     auto Pc = [&](double a, double b, double c, double d, double e, double f, double* U) {

@@ -197,7 +197,7 @@ int cfd_settings_ic(const cfd_settings* s, const cfd_config* cfg, double* grid) 
     return cfd_case_ic(cfg, s->test_case, s->seed, grid);
 }
 
-// E/sourcecode/euler_io.cpp:1188-1216, A/sourcecode/allaire_diffuse_io.cpp:1153-1186
+// E/sourcecode/euler_io.cpp:1188-1216, A/sourcecode/allaire_diffuse_io.cpp:1155-1186
 int cfd_write_state(const cfd_config* c, const double* grid, const char* basename, double t) {
     if (!c || !grid || !basename) return cfd_fail(CFD_ERR_INVALID, "cfd_write_state: null argument");
     View v = view_of(c, grid);

@@ -121,7 +121,7 @@ int cfd_upload_device(cfd_solver* s, const double* dev_soa, int n, double t);
 /* Builds the initial condition on the device, straight into the solver's
  * state: a seeded recipe (CFD_RECIPE_*, declared in cfdgpu_host.h) or a named
  * reference test case (set_ICs, sourcecode/euler_io.cpp:436-731 and
- * A/sourcecode/allaire_diffuse_io.cpp:401-640).  The result is bit-identical
+ * A/sourcecode/allaire_diffuse_io.cpp:402-640).  The result is bit-identical
  * to cfd_recipe_ic / cfd_case_ic followed by cfd_upload, without a host grid
  * or a host-to-device copy of the state.  The four Allaire cases with
  * per-cell formulas (shocked_SF6, TSTM, RMI_SF6, tin_air_implosion) return

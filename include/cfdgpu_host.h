@@ -76,7 +76,7 @@ int cfd_settings_ic(const cfd_settings* s, const cfd_config* cfg, double* grid);
 
 /* Output writers in the reference formats, from a ghosted AoS grid:
  *   <basename>-state-<t>.dat       (E/sourcecode/euler_io.cpp:1188-1216,
- *                                   A/sourcecode/allaire_diffuse_io.cpp:1153-1186)
+ *                                   A/sourcecode/allaire_diffuse_io.cpp:1155-1186)
  *   <basename>-schlieren-<t>.dat   (E: :1142-1185)
  * with <t> formatted like std::to_string(double). */
 int cfd_write_state(const cfd_config* cfg, const double* grid, const char* basename, double t);

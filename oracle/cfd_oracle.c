@@ -424,7 +424,7 @@ static void set_bcs(const eosp* q, const ref_params* p, grid_t* G) {
         }
 }
 
-/* E/sourcecode/euler_rowsweep.cpp:47-82 (and euler_colsweep.cpp:173-208):
+/* E/sourcecode/euler_rowsweep.cpp:47-82 (and euler_colsweep.cpp:78-113):
  * restore rho or e from the old state when the update made them <= 1e-12. */
 static void euler_fixup(const eosp* q, double* f, const double* old) {
     if (is_phys(q, f)) return;
