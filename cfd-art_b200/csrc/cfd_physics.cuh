@@ -123,7 +123,7 @@ __device__ __forceinline__ void cons_to_prim(const Eos& q, const double* U, Prim
     }
 }
 
-// E/headers/misc_euler.hpp:83-97 / A/headers/misc.hpp:149-163.
+// E/headers/misc_euler.hpp:82-97 / A/headers/misc.hpp:149-163.
 // Returns the specific internal energy it used through e_out.
 template <int MODEL>
 __device__ __forceinline__ void prim_to_cons(const Eos& q, const double* W, double* U,
@@ -447,7 +447,7 @@ __device__ __forceinline__ void hllc_flux(const Eos& q, int wavespeed, const dou
     if constexpr (MODEL == MODEL_ALLAIRE) F[5] = 0.0;
 }
 
-// Allaire z-update (A/headers/zupdate.hpp:26-30 upwind, :44-49 second order);
+// Allaire z-update (A/headers/zupdate.hpp:44-49 upwind, :62-67 second order);
 // z_min > 0 clips to [z_min, 1 - z_min] instead of [0, 1].
 __device__ __forceinline__ double z_update(bool godunov, double k, double zL, double z, double zR,
                                            double usL, double usR, double zsL, double zsR,

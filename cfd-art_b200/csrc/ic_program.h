@@ -60,7 +60,7 @@ struct Geom {
     double x0, y0, dx, dy;
 };
 
-// E/headers/misc_euler.hpp:83-97
+// E/headers/misc_euler.hpp:82-97
 IC_HD void euler_p2c(const Eos& q, const double* W, double* U) {
     double rho = W[0], u = W[1], v = W[2], p = W[3];
     double e = (p + q.g1 * q.p1) / ((q.g1 - 1.0) * rho);

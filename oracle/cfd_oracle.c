@@ -96,7 +96,7 @@ static void c2p(const eosp* q, const double* U, double* W) {
     }
 }
 
-/* E/headers/misc_euler.hpp:83-97, A/headers/misc.hpp:149-163 */
+/* E/headers/misc_euler.hpp:82-97, A/headers/misc.hpp:149-163 */
 static void p2c(const eosp* q, const double* W, double* U) {
     if (q->model == ORACLE_EULER) {
         double rho = W[0], u = W[1], v = W[2], p = W[3];
@@ -442,7 +442,7 @@ static void euler_fixup(const eosp* q, double* f, const double* old) {
     p2c(q, W, f);
 }
 
-/* A/headers/zupdate.hpp:26-30 (upwind) and :44-49 (second order), with the
+/* A/headers/zupdate.hpp:44-49 (upwind) and :62-67 (second order), with the
  * hook clip interval [z_min, 1-z_min] (z_min = 0 is the reference). */
 static double zupdate(const ref_params* p, double dx, double dt, double zL, double z, double zR,
                       double usL, double usR, double zsL, double zsR) {
