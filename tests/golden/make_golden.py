@@ -3,6 +3,7 @@
     python tests/golden/make_golden.py            # everything
     python tests/golden/make_golden.py outputs    # only the whole-run output files
     python tests/golden/make_golden.py adapter    # only the adapter's extra runs (golden/adapter/)
+    python tests/golden/make_golden.py --out DIR  # everything, written under DIR instead
 
 Requires oracle/_ref/libref_{euler,allaire}.so (built by `make -C oracle ref`
 from the reference sources) and cfd-art_b200/lib/libcfdgpu.so (only for the
@@ -20,6 +21,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
+OUT = HERE  # where fixtures are written (--out DIR: elsewhere, e.g. to compare)
 sys.path.insert(0, str(ROOT / "oracle"))
 sys.path.insert(0, str(ROOT / "cfd-art_b200"))
 
@@ -62,7 +64,7 @@ def save(name, model, ic, grid, p, taken, n, t, dts, store_full=True):
         out["state"] = fin
     for k, v in params_dict(p).items():
         out["p_" + k] = np.array(v)
-    np.savez_compressed(HERE / f"{name}.npz", **out)
+    np.savez_compressed(OUT / f"{name}.npz", **out)
     print(f"{name}: {taken} steps, t={t:.6g}, sha256={digest(fin)[:16]}")
 
 
@@ -100,7 +102,7 @@ def kat_faces(model, nfaces, seed):
         F[f] = fl
         us[f] = a
         zs[f] = b if b is not None else 0.0
-    np.savez_compressed(HERE / f"kat_faces_{model}.npz", stencils=U, flux=F, u_star=us,
+    np.savez_compressed(OUT / f"kat_faces_{model}.npz", stencils=U, flux=F, u_star=us,
                         z_star=zs, dt=np.array(dt), dx=np.array(dx),
                         **{"p_" + k: np.array(v) for k, v in params_dict(p).items()})
     print(f"kat_faces_{model}: {nfaces} faces")
@@ -159,8 +161,8 @@ OUTPUT_RUNS = [
 
 # More whole runs, for the reference-loop adapter's CPU check only (kept in
 # golden/adapter/ so that the GPU driver test does not collect them): the
-# Godunov scheme (one ghost layer), Strang splitting for Euler, naive
-# splitting for Allaire.
+# Godunov scheme (one ghost layer) for both models, Strang splitting for
+# Euler, naive splitting for Allaire.
 ADAPTER_RUNS = [
     ("godunov_totem_pole_2_20x20", "euler",
      "Nx 20\nNy 20\nCFL 0.5\nsplitting_scheme naive_splitting\ntest_case totem_pole_2\n"
@@ -177,7 +179,8 @@ ADAPTER_RUNS = [
 ]
 
 
-def output_run(name: str, model: str, settings: str, dest: Path = HERE) -> None:
+def output_run(name: str, model: str, settings: str, dest: Path | None = None) -> None:
+    dest = OUT if dest is None else dest
     import os
     import subprocess
     import tempfile
@@ -199,13 +202,18 @@ def output_run(name: str, model: str, settings: str, dest: Path = HERE) -> None:
 
 
 if __name__ == "__main__":
-    if sys.argv[1:] == ["outputs"]:
+    args = sys.argv[1:]
+    if args[:1] == ["--out"]:
+        OUT = Path(args[1]).resolve()
+        OUT.mkdir(parents=True, exist_ok=True)
+        args = args[2:]
+    if args == ["outputs"]:
         for run in OUTPUT_RUNS:
             output_run(*run)
-    elif sys.argv[1:] == ["adapter"]:
+    elif args == ["adapter"]:
         for run in ADAPTER_RUNS:
-            output_run(*run, dest=HERE / "adapter")
+            output_run(*run, dest=OUT / "adapter")
     else:
         main()
         for run in ADAPTER_RUNS:
-            output_run(*run, dest=HERE / "adapter")
+            output_run(*run, dest=OUT / "adapter")
