@@ -92,16 +92,21 @@ typedef struct cfd_status {
 
 typedef struct cfd_solver cfd_solver;
 
-/* Library identification (build string). */
+/* Library identification (build string).  No counterpart in the reference. */
 const char* cfd_version(void);
 
-/* Message of the last failing call on this thread; returns its length. */
+/* Message of the last failing call on this thread; returns its length.
+ * Replaces the reference's assert aborts and printed messages (e.g.
+ * sourcecode/euler_io.cpp:232). */
 int cfd_last_error(char* buf, size_t len);
 
-/* Number of stored components per cell for a model (4 or 6). */
+/* Number of stored components per cell for a model (4 or 6): the vectype
+ * size of gridtype (sourcecode/euler_io.cpp:494, A/sourcecode/
+ * allaire_diffuse_io.cpp:462). */
 int cfd_nvar(int model);
 
-/* Bytes of device memory cfd_create would allocate for cfg. */
+/* Bytes of device memory cfd_create would allocate for cfg.  No counterpart
+ * in the reference (host memory only). */
 int cfd_device_bytes(const cfd_config* cfg, size_t* bytes);
 
 /* Allocates a solver and its device state.  Replaces problem->set_ICs'
@@ -112,10 +117,12 @@ int cfd_destroy(cfd_solver* s);
 
 /* Copies an initial condition to the device and computes the wave speeds of
  * it.  `host` is read in `layout`; ghost cells are ignored (they are rebuilt
- * by every sweep, as pre_sweep does).  n and t set the step count and time. */
+ * by every sweep, as pre_sweep does).  n and t set the step count and time.
+ * Replaces handing set_ICs' grid to the time loop (headers/simulation.hpp:39-40). */
 int cfd_upload(cfd_solver* s, const double* host, int layout, int n, double t);
 
-/* Same from device memory (SoA planes of nx*ny doubles each, nvar planes). */
+/* Same from device memory (SoA planes of nx*ny doubles each, nvar planes).
+ * No counterpart in the reference. */
 int cfd_upload_device(cfd_solver* s, const double* dev_soa, int n, double t);
 
 /* Builds the initial condition on the device, straight into the solver's
@@ -131,7 +138,8 @@ int cfd_upload_recipe(cfd_solver* s, int recipe, uint64_t seed, int nbubbles, in
 int cfd_upload_case(cfd_solver* s, const char* test_case, uint64_t seed, int n, double t);
 
 /* Copies the current state to the host in `layout`.  In the ghosted layout
- * the ghost strips hold the boundary fill of the current state. */
+ * the ghost strips hold the boundary fill of the current state.  Replaces
+ * reading the grid that problem->output gets (headers/simulation.hpp:50, :65). */
 int cfd_download(cfd_solver* s, double* host, int layout);
 /* Schlieren field of the current state computed on the device: |grad rho|
  * of every interior cell by central differences, as the reference's writer
@@ -184,10 +192,13 @@ int cfd_step(cfd_solver* s, double dt);
  * t >= T.  Asynchronous; steps past the end are no-ops. */
 int cfd_advance(cfd_solver* s, int max_steps);
 
-/* Waits for the solver's stream and returns the time-loop state. */
+/* Waits for the solver's stream and returns the time-loop state: the n and t
+ * that headers/simulation.hpp:44-61 keeps on the host, with the masses
+ * compute_dt records (sourcecode/euler_timestep.cpp:31-32) and the counters. */
 int cfd_get_status(cfd_solver* s, cfd_status* st);
 
-/* Kernel timing for profiling: while enabled, every sweep launch is
+/* Kernel timing for profiling (no counterpart: the reference times the whole
+ * run, sourcecode/main.cpp:39-43): while enabled, every sweep launch is
  * bracketed by CUDA events on the solver's stream (steps launch one by one
  * instead of from the captured graph).  cfd_kernel_times returns the summed
  * durations (ms) and launch counts per sweep direction (0: x, 1: y) since
@@ -196,14 +207,17 @@ int cfd_set_kernel_timing(cfd_solver* s, int enable);
 int cfd_kernel_times(cfd_solver* s, double ms[2], int launches[2]);
 int cfd_reset_kernel_times(cfd_solver* s);
 
-/* Resets the event counters. */
+/* Resets the event counters (the reference prints each event instead,
+ * e.g. sourcecode/euler_rowsweep.cpp:51). */
 int cfd_reset_counters(cfd_solver* s);
 
-/* Waits for all work queued on the solver's stream. */
+/* Waits for all work queued on the solver's stream.  No counterpart in the
+ * reference. */
 int cfd_synchronize(cfd_solver* s);
 
 /* Device-side layout of the current state for zero-copy callers: SoA planes
- * `plane` elements apart, rows `pitch` elements apart, FP64. */
+ * `plane` elements apart, rows `pitch` elements apart, FP64.  No counterpart
+ * in the reference. */
 int cfd_state_device(cfd_solver* s, const void** dev_ptr, int64_t* plane, int* pitch);
 
 /* compute_dt without any device allocation, for callers that may not call
@@ -332,6 +346,8 @@ typedef struct cfd_server_stats {
 } cfd_server_stats;
 
 typedef struct cfd_server cfd_server;
+/* Creates a server and starts its worker thread.  No counterpart in the
+ * reference, which runs one problem per process (sourcecode/main.cpp:17-48). */
 int cfd_server_create(const cfd_server_options* opt, cfd_server** out);
 /* Queues a solve of `steps` steps (or to cfg.T) from a ghosted AoS initial
  * grid, which is copied; CFD_ERR_BUDGET if it can never fit. */

@@ -21,7 +21,8 @@ enum {
     CFD_RECIPE_WATER_SHOCK_AIR_BUBBLE = 3 /* Allaire: 1e9 Pa water shock on an air bubble, [0,2]x[0,1] */
 };
 
-/* Doubles in a ghosted AoS grid for cfg. */
+/* Doubles in a ghosted AoS grid for cfg: the size of the reference's
+ * gridtype (sourcecode/euler_io.cpp:494). */
 int cfd_ic_grid_elems(const cfd_config* cfg, size_t* elems);
 
 /* set_parameters of a named reference test case
@@ -32,11 +33,13 @@ int cfd_case_config(int model, const char* test_case, int nx, int ny, int flux_s
                     cfd_config* cfg);
 
 /* set_ICs of a named reference test case into `grid` (ghosted AoS, ghosts
- * included as the reference fills them).  `seed` is used only by the Euler
- * case "internet", which the reference seeds from std::random_device. */
+ * included as the reference fills them; E/sourcecode/euler_io.cpp:436-731,
+ * A/sourcecode/allaire_diffuse_io.cpp:402-990).  `seed` is used only by the
+ * Euler case "internet", which the reference seeds from std::random_device. */
 int cfd_case_ic(const cfd_config* cfg, const char* test_case, uint64_t seed, double* grid);
 
-/* Configuration and initial condition of a seeded recipe. */
+/* Configuration and initial condition of a seeded recipe.  No counterpart in
+ * the reference: these are the benchmark workloads' initial conditions. */
 int cfd_recipe_config(int recipe, int nx, int ny, cfd_config* cfg);
 int cfd_recipe_ic(const cfd_config* cfg, int recipe, uint64_t seed, int nbubbles, double* grid);
 
@@ -66,11 +69,14 @@ typedef struct cfd_settings {
     int nbubbles;
 } cfd_settings;
 
+/* Parses a settings file (headers/settings_file.hpp:35-71, basename as :69). */
 int cfd_read_settings(const char* path, cfd_settings* out);
 
 /* Fills a solver configuration (and the initial grid when grid != NULL) from
  * settings: a reference test case name or a recipe name
- * ("four_quadrant", "shock_bubbles", "water_shock_air_bubble"). */
+ * ("four_quadrant", "shock_bubbles", "water_shock_air_bubble").  Replaces
+ * set_ICs' reading of the settings (E/sourcecode/euler_io.cpp:436-461) and
+ * set_splitting_scheme (headers/splitting_scheme.hpp:125-143). */
 int cfd_settings_config(const cfd_settings* s, cfd_config* cfg);
 int cfd_settings_ic(const cfd_settings* s, const cfd_config* cfg, double* grid);
 
