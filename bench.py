@@ -208,6 +208,15 @@ def build_ic(G, recipe, nx, ny, seed, nbub):
 
 # ------------------------------------------------------------ CPU baseline --
 
+def _host_threads() -> int:
+    """Host CPUs this process may run on (its affinity mask, which a container
+    or a scheduler may narrow below the machine's count)."""
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
 def _cpu_model() -> str:
     """The host CPU's model name (first entry of /proc/cpuinfo)."""
     try:
@@ -247,7 +256,7 @@ def cpu_baseline(workload: str, budget_s: float = 16.0, single_thread_s: float =
     import cfdgpu as G
     import oracle_py as O
 
-    cores = os.cpu_count() or 1
+    cores = _host_threads()
     if not (O.ref_available("euler") and O.ref_available("allaire")):
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                 "sample": "unavailable: oracle/_ref (reference build) absent"}
@@ -301,7 +310,7 @@ def run_reference(args) -> None:
         return
     import cfdgpu as G
 
-    cores = os.cpu_count() or 1
+    cores = _host_threads()
     w = args.workload
     parts = []
     if w in ("served", "batch256") or w.startswith("euler"):
