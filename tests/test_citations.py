@@ -52,7 +52,8 @@ def test_cited_line_ranges_exist():
     if r.returncode == 0:
         files = r.stdout.split()
     else:  # a copy without git history: every file outside the scratch and build trees
-        skip = ("_work/", "gpurun_out/", "oracle/_ref/", "oracle/_build/", "cfd-art_b200/lib/")
+        skip = ("_work/", "gpurun_out/", "baseline/", "oracle/_ref/", "oracle/_build/",
+                "cfd-art_b200/lib/")
         files = [str(p.relative_to(ROOT)) for p in ROOT.rglob("*") if p.is_file()]
         files = [f for f in files if not f.startswith(skip) and "/." not in "/" + f]
     bad = []
