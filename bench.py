@@ -168,6 +168,20 @@ def _rel_linf_density(a: np.ndarray, b: np.ndarray, model: int) -> float:
     return float(np.abs(ra - rb).max() / np.abs(rb).max())
 
 
+def _errors(a: np.ndarray, b: np.ndarray, model: int) -> tuple[float, float]:
+    return _rel_l1_density(a, b, model), _rel_linf_density(a, b, model)
+
+
+def _error_summary(pairs, basis: str) -> dict:
+    """Relative L1 and L-inf density errors of a set of results: largest and
+    median, with what they were measured against."""
+    l1 = [a for a, _ in pairs]
+    li = [b for _, b in pairs]
+    return {"l1": {"max": max(l1), "median": float(np.median(l1)), "bound": 1e-4},
+            "linf": {"max": max(li), "median": float(np.median(li))}, "results": len(pairs),
+            "basis": basis}
+
+
 # ------------------------------------------------------- request streams --
 
 def served_requests(n: int, seed: int):
@@ -230,118 +244,165 @@ def _cpu_model() -> str:
     return platform.processor() or "unknown"
 
 
-def _ref_rate(O, G, recipe, n_x, n_y, nbub, budget_s, cores):
-    import ctypes
+# Cell-updates per reference-arm unit: a request or instance runs at most
+# this many cell-updates (its own step count, truncated), so one unit takes
+# a few seconds of host time.
+REF_UNIT_CELLS = {"euler": 1.6e7, "allaire": 6e6}
 
-    model = "euler" if recipe == "shock_bubbles" else "allaire"
-    cfg, ic = build_ic(G, recipe, n_x, n_y, SEED, nbub)
-    p = O.make_params(n_x, n_y, cfg.dx, cfg.dy, cfg.gamma1, cfg.pinf1, cfg.gamma2, cfg.pinf2,
-                      bc=tuple(cfg.bc), cfl=cfg.cfl, T=cfg.T, limiter=cfg.limiter,
-                      wavespeed=cfg.wavespeed, z_min=cfg.z_min)
-    lib = O.ref_lib(model)
-    f = getattr(lib, f"ref_{model}_last_loop_seconds")
-    f.restype = ctypes.c_double
-    g = ic.copy()
-    O.ref_run(model, p, g, 1, threads=cores)
-    t1 = f()
-    steps = max(2, min(60, int(budget_s / max(t1, 1e-3))))
-    taken, _, _, _ = O.ref_run(model, p, g, steps, n=1, threads=cores)
-    return n_x * n_y * taken, f(), taken
+
+def reference_units(workload: str, count: int):
+    """The workload's units as the reference's CPU code runs them:
+    (recipe, nx, ny, seed, nbubbles, steps).  served: the repo arm's request
+    stream (same seeds; warm-up requests first); batch256: its instances;
+    single-grid workloads: the grid itself, `steps` = 1 per unit."""
+    if workload == "served":
+        return [(rec, nx, ny, sd, nb, steps)
+                for (_, rec, nx, ny, steps, sd, nb) in served_requests(count, SEED)]
+    if workload == "batch256":
+        return [(r, nx, ny, sd, nb, steps)
+                for r, nx, ny, steps, sd, nb in batch_instances(256, SEED)][:count]
+    recipe, nx, ny, nbub, _prec = SINGLE[workload]
+    return [(recipe, nx, ny, SEED, nbub, 1)]
+
+
+class RefRunner:
+    """The reference's own CPU implementation of the path (oracle/_ref: its
+    sources built here) driven through its time loop on grids that the
+    CPU-side recipe builder makes (oracle/oracle_recipes.c), so the shipped
+    library is never loaded on this arm.  Returns cell-updates and the loop's
+    own seconds (the reference's omp_get_wtime around the loop)."""
+
+    def __init__(self, threads: int):
+        import ctypes
+
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle_py as O
+
+        self.O, self.threads = O, threads
+        self.secs = {}
+        for model in ("euler", "allaire"):
+            f = getattr(O.ref_lib(model), f"ref_{model}_last_loop_seconds")
+            f.restype = ctypes.c_double
+            self.secs[model] = f
+
+    def unit(self, recipe, nx, ny, seed, nb, steps, cap=True):
+        grid, p, model = self.O.port_recipe_ic(recipe, nx, ny, seed, nb)
+        if cap:
+            steps = max(2, min(steps, int(REF_UNIT_CELLS[model] // (nx * ny))))
+        taken, _, _, _ = self.O.ref_run(model, p, grid, steps, threads=self.threads)
+        return nx * ny * taken, self.secs[model](), taken, model
+
+    def grid_steps(self, recipe, nx, ny, seed, nb, warm, steps):
+        """Single-grid workloads: `warm` steps, then `steps` timed ones, one
+        timing per step."""
+        grid, p, model = self.O.port_recipe_ic(recipe, nx, ny, seed, nb)
+        if warm:
+            self.O.ref_run(model, p, grid, warm, threads=self.threads)
+        out, n = [], warm
+        for _ in range(steps):
+            taken, n, _, _ = self.O.ref_run(model, p, grid, 1, n=n, threads=self.threads)
+            out.append((nx * ny * taken, self.secs[model]()))
+        return out
+
+
+def _ref_available() -> bool:
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle_py as O
+
+    return O.ref_available("euler") and O.ref_available("allaire") and O.port_available()
 
 
 def cpu_baseline(workload: str, budget_s: float = 16.0, single_thread_s: float = 5.0) -> dict:
     """The reference's own CPU code (oracle/_ref, all host threads) on a
-    bounded sample of the workload, plus a one-thread run (`single_thread`)."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import cfdgpu as G
-    import oracle_py as O
-
-    cores = _host_threads()
-    if not (O.ref_available("euler") and O.ref_available("allaire")):
+    bounded sample of the workload's units, plus a one-thread run
+    (`single_thread`, deterministic: with more threads the reference's
+    compute_dt races on its maxima) on units cut to a quarter of the size."""
+    if not _ref_available():
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                 "sample": "unavailable: oracle/_ref (reference build) absent"}
-    parts = []
-    if workload in ("served", "batch256") or workload.startswith("euler"):
-        parts.append(("shock_bubbles", 1024, 1024, 32, 0.7 if workload == "served" else 1.0))
-    if workload == "served" or workload.startswith("allaire"):
-        parts.append(("water_shock_air_bubble", 512, 256, 1, 0.3 if workload == "served" else 1.0))
-    cells = secs = 0.0
-    desc = []
-    for recipe, nx, ny, nb, share in parts:
-        c, s, k = _ref_rate(O, G, recipe, nx, ny, nb, budget_s * share, cores)
-        cells += c
-        secs += s
-        desc.append(f"{recipe} {nx}x{ny} x {k} steps")
-    out = {"value": cells / secs / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
-           "cpu_model": _cpu_model(),
-           "sample": "; ".join(desc) + f" ({cores} OpenMP threads, time loop only, {secs:.1f} s)"}
-    # The same code on one thread (deterministic: with more threads the
-    # reference's compute_dt races on its maxima), on a smaller sample of the
-    # same recipes so that it stays within a few seconds.
-    cells = secs = 0.0
-    desc = []
-    for recipe, nx, ny, nb, share in parts:
-        sx, sy = (256, 256) if recipe == "shock_bubbles" else (256, 128)
-        c, s, k = _ref_rate(O, G, recipe, sx, sy, nb, single_thread_s * share, 1)
-        cells += c
-        secs += s
-        desc.append(f"{recipe} {sx}x{sy} x {k} steps")
-    out["single_thread"] = {"value": cells / secs / 1e9, "unit": UNIT, "cores": 1,
-                            "sample": "; ".join(desc) + f" (1 thread, time loop only, "
-                                                        f"{secs:.1f} s)"}
+    cores = _host_threads()
+    out = {}
+    for threads, budget, shrink in ((cores, budget_s, 1), (1, single_thread_s, 4)):
+        R = RefRunner(threads)
+        cells = secs = 0.0
+        units = taken_steps = 0
+        for (rec, nx, ny, sd, nb, steps) in reference_units(workload, 64):
+            nx, ny = max(16, nx // shrink), max(16, ny // shrink)
+            if workload in SINGLE:
+                c, s, k, _ = R.unit(rec, nx, ny, sd, nb, 1 << 30)
+            else:
+                c, s, k, _ = R.unit(rec, nx, ny, sd, nb, steps)
+            cells += c
+            secs += s
+            units += 1
+            taken_steps += k
+            if secs >= budget:
+                break
+        what = ("requests" if workload == "served" else
+                "instances" if workload == "batch256" else "grid runs")
+        desc = (f"first {units} {what} of the {workload} workload"
+                + (f" at 1/{shrink} size per side" if shrink > 1 else "")
+                + f", each truncated to <= {REF_UNIT_CELLS['euler']:.2g} (Euler) / "
+                  f"{REF_UNIT_CELLS['allaire']:.2g} (Allaire) cell-updates, {taken_steps} steps "
+                  f"in all ({threads} OpenMP thread{'s' if threads > 1 else ''}, time loop only, "
+                  f"{secs:.1f} s)")
+        rec = {"value": cells / secs / 1e9, "unit": UNIT, "cores": threads, "sample": desc}
+        if threads == cores:
+            out = {**rec, "kind": "reference", "cpu_model": _cpu_model()}
+        else:
+            out["single_thread"] = rec
     return out
 
 
 def run_reference(args) -> None:
     """Reference arm: the reference's CPU implementation (oracle/_ref: its
-    own sources built here) on a bounded sample of the workload, one time
-    step per bench step, all host threads."""
+    own sources built here) with all host threads, on the repo arm's
+    workload, with the shipped library never loaded.  One bench step is one
+    unit of the workload: served, a request of the same seeded stream (its
+    own step count, truncated to a few seconds of host work); batch256, an
+    instance; single-grid workloads, one time step of the full grid."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import ctypes
-
-    import oracle_py as O
-
     base = {"impl": "reference", "metric": METRIC, "unit": UNIT}
-    if not (O.ref_available("euler") and O.ref_available("allaire")):
+    if not _ref_available():
         print(json.dumps({**base, "unavailable": "oracle/_ref (reference build) absent"}))
         return
-    import cfdgpu as G
-
     cores = _host_threads()
-    w = args.workload
-    parts = []
-    if w in ("served", "batch256") or w.startswith("euler"):
-        parts.append(("euler", "shock_bubbles", 512, 512, 32))
-    if w == "served" or w.startswith("allaire"):
-        parts.append(("allaire", "water_shock_air_bubble", 256, 128, 1))
+    R = RefRunner(cores)
+    w, K, W = args.workload, args.steps, args.warmup
     cells = secs = 0.0
-    for model, recipe, nx, ny, nb in parts:
-        cfg, ic = build_ic(G, recipe, nx, ny, SEED, nb)
-        p = O.make_params(nx, ny, cfg.dx, cfg.dy, cfg.gamma1, cfg.pinf1, cfg.gamma2, cfg.pinf2,
-                          bc=tuple(cfg.bc), cfl=cfg.cfl, T=cfg.T, limiter=cfg.limiter,
-                          wavespeed=cfg.wavespeed, z_min=cfg.z_min)
-        f = getattr(O.ref_lib(model), f"ref_{model}_last_loop_seconds")
-        f.restype = ctypes.c_double
-        g = ic.copy()
-        if args.warmup:
-            O.ref_run(model, p, g, args.warmup, threads=cores)
-        taken, _, _, _ = O.ref_run(model, p, g, args.steps, n=args.warmup, threads=cores)
-        cells += nx * ny * taken
-        secs += f()
+    if w in SINGLE:
+        rec, nx, ny, sd, nb, _ = reference_units(w, 1)[0]
+        for c, s in R.grid_steps(rec, nx, ny, sd, nb, W, K):
+            cells += c
+            secs += s
+        sample = f"{rec} {nx}x{ny}: {W} warm-up steps, then {K} timed steps"
+    else:
+        units = reference_units(w, W + K)
+        for u in units[:W]:
+            R.unit(*u)
+        taken_steps = 0
+        for u in units[W:W + K]:
+            c, s, k, _ = R.unit(*u)
+            cells += c
+            secs += s
+            taken_steps += k
+        sample = (f"{'requests' if w == 'served' else 'instances'} {W + 1}-{W + K} of the "
+                  f"{w} workload's seeded list (after {W} warm-up ones), each run from its "
+                  f"initial grid for its own step count truncated to <= "
+                  f"{REF_UNIT_CELLS['euler']:.2g} (Euler) / {REF_UNIT_CELLS['allaire']:.2g} "
+                  f"(Allaire) cell-updates: {taken_steps} steps in all")
     val = cells / secs / 1e9
-    sample = (" + ".join(f"{r} {nx}x{ny}" for _, r, nx, ny, _ in parts) +
-              f", {args.steps} steps each, {cores} OpenMP threads, time loop only")
+    sample += f"; {cores} OpenMP threads, the reference's time loop only ({secs:.1f} s)"
     print(json.dumps({
-        **base, "value": val, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * secs / max(args.steps, 1), "higher_is_better": True,
+        **base, "value": val, "n_gpus": args.gpus, "steps": K, "warmup": W,
+        "ms_per_step": 1e3 * secs / max(K, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": w, "sample": sample},
+        "config": {"workload": w, "step": "one request" if w == "served" else
+                   "one instance" if w == "batch256" else "one time step", "sample": sample},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "cpu_model": _cpu_model(),
-                         "sample": sample},
+                         "cpu_model": _cpu_model(), "sample": sample},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -443,6 +504,9 @@ def bench_single(args, ctx, G, stream, clocks):
     e2e = None
     if not args.no_e2e:
         e2e = e2e_single(G, torch, cfg, ic, K, W, ctx, prec)
+    acc = None
+    if prec == "mixed" and not args.no_accuracy:
+        acc = accuracy_single(G, cfg, ic, STATED_STEPS.get(recipe, K))
     value = job_throughput(ctx, cells * K, ms)
     config = {"workload": args.workload, "model": model, "precision": prec, "grid": [nx, ny],
               "bubbles": nbub, "seed": SEED, "cfl": cfg.cfl,
@@ -451,7 +515,33 @@ def bench_single(args, ctx, G, stream, clocks):
               "parallelism": f"replicas x{ctx.world}"}
     return {"value": value, "ms_per_step": ms / K,
             "dtype": "f64" if prec == "fp64" else "f32+f32comp", "config": config, "clocks": ck,
-            "gpu_launches": launches, "roofline": rl, "e2e": e2e, "sim": {"n": st.n, "t": st.t}}
+            "gpu_launches": launches, "roofline": rl, "e2e": e2e, "sim": {"n": st.n, "t": st.t},
+            **({"accuracy_vs_fp64": acc} if acc else
+               {"accuracy_vs_fp64": {"l1": {"max": 0.0}, "linf": {"max": 0.0},
+                                     "basis": "bit-identical to the oracle and the reference "
+                                              "build (tests/test_gpu_parity.py)"}}
+               if prec == "fp64" else {})}
+
+
+# the stated step counts of the benchmarked configurations
+STATED_STEPS = {"shock_bubbles": 2000, "water_shock_air_bubble": 1500}
+
+
+def accuracy_single(G, cfg, ic, steps) -> dict:
+    """Mixed vs plain FP64 (bit-identical to the reference) on the bench's
+    grid over the configuration's stated step count, outside the timed
+    region."""
+    with G.Solver(cfg) as s:
+        s.upload(ic)
+        s.advance(steps)
+        ref = s.download()
+    with G.Batch(stream=cfg.stream) as b:
+        i = b.add(cfg, ic, steps)
+        b.step(steps)
+        out = b.download(i)
+        n = b.status(i).n
+    return {**_error_summary([_errors(out, ref, cfg.model)],
+                             "plain FP64 form, bit-identical to the reference"), "steps": n}
 
 
 def e2e_single(G, torch, cfg, ic, K, W, ctx, prec) -> dict:
@@ -546,7 +636,25 @@ def bench_batch(args, ctx, G, stream, clocks):
         e2e = {"value": ctx.sum(upd2) / secs / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": nbytes / K, "d2h_bytes_per_step": nbytes / K, "seconds": secs}
         del outs, pins
+    acc = None
+    if not args.no_accuracy:
+        # every instance to its 500 steps, mixed vs plain FP64
+        outs = {}
+        with G.Batch(stream=stream.cuda_stream) as b3:
+            ids = [b3.add(c, ic, inst[3]) for (c, ic), inst in zip(ics, insts)]
+            b3.step(max(i[3] for i in insts))
+            for k, i in enumerate(ids):
+                outs[k] = b3.download(i)
+        pairs = []
+        for k, ((c, ic), inst) in enumerate(zip(ics, insts)):
+            with G.Solver(c) as s1:
+                s1.upload(ic)
+                s1.advance(inst[3])
+                pairs.append(_errors(outs[k], s1.download(), c.model))
+        acc = {**_error_summary(pairs, "plain FP64 form, bit-identical to the reference"),
+               "steps": insts[0][3]}
     return {"value": value, "ms_per_step": ms / K, "dtype": "f32+f32comp",
+            "accuracy_vs_fp64": acc,
             "config": {"workload": "batch256", "model": "euler", "precision": "mixed",
                        "instances": 256, "cells": cells, "sizes": "nx, ny log-uniform [64, 1024]",
                        "bubbles": "4-16 per instance", "steps_per_instance": 500,
@@ -589,7 +697,7 @@ def _serve(G, reqs, ics, precision, ticks, stream):
 
 def bench_served(args, ctx, G, stream, clocks):
     torch = ctx.torch
-    K, W = max(args.steps, 4), args.warmup
+    K, W = max(args.steps, 1), args.warmup
     reqs = served_requests(W + K, SEED + 7919 * ctx.rank)
     t_ic = time.perf_counter()
     ics = [build_ic(G, rec, nx, ny, sd, nb) for (_, rec, nx, ny, steps, sd, nb) in reqs]
@@ -653,8 +761,9 @@ def bench_served(args, ctx, G, stream, clocks):
     fp64_val = ctx.sum(upd) / ctx.max(mk_f) / 1e9
     models = 1 + any(r[1] != "shock_bubbles" for r in timed)
     return {
-        "value": value, "ms_per_step": ms / max_steps, "dtype": "f32+f32comp",
-        "config": {"workload": "served", "requests": len(timed), "warmup_requests": W,
+        "value": value, "ms_per_step": ms / len(timed), "dtype": "f32+f32comp",
+        "config": {"workload": "served", "step": "one request (ms_per_step: device ms of the "
+                   "resident run per timed request)", "requests": len(timed), "warmup_requests": W,
                    "arrivals": "Poisson, mean 50/s, seeded",
                    "mix": "70% Euler shock_bubbles, 30% Allaire water_shock_air_bubble "
                           "(PVRS, alpha clip 1e-6)",
@@ -690,6 +799,8 @@ def main() -> None:
     ap.add_argument("--workload", default="served", choices=WORKLOADS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling)")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the mixed-vs-FP64 error runs (profiling)")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 48 if args.workload == "served" else 50
@@ -697,6 +808,17 @@ def main() -> None:
         args.warmup = 4 if args.workload == "served" else 5
     if args.impl == "ours" and args.warmup < 3:
         args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "0"))
+    if world == 0 and args.gpus > 1:
+        # one process per GPU: relaunch under torchrun with the same arguments
+        port = 29500 + os.getpid() % 2000
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+               f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+               "--master-port", str(port), str(Path(__file__).resolve()), *sys.argv[1:]]
+        os.execv(sys.executable, cmd)
+    world = max(world, 1)
+    if world != args.gpus:
+        sys.exit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; launch one rank per GPU")
     if args.impl == "reference":
         run_reference(args)
         return
@@ -707,7 +829,6 @@ def main() -> None:
     import cfdgpu as G
 
     rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     if world > 1:

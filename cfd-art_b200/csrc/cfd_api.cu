@@ -17,6 +17,7 @@
 
 #include "../../include/cfdgpu.h"
 #include "cfd_checkpoint.h"
+#include "cfd_config.h"
 #include "cfd_error.h"
 #include "cfd_frame.h"
 #include "cfd_ic.h"
@@ -124,9 +125,10 @@ struct cfd_solver {
     int ev_n[2] = {0, 0};
 };
 
-namespace {
+namespace cfd {
 
-int validate(const cfd_config* c) {
+// cfd_create's checks of a configuration (cfd_config.h).
+int validate_config(const cfd_config* c) {
     if (!c) return fail(CFD_ERR_INVALID, "null config");
     if (c->model != CFD_MODEL_EULER && c->model != CFD_MODEL_ALLAIRE)
         return fail(CFD_ERR_INVALID, "unknown model %d", c->model);
@@ -171,6 +173,10 @@ Eos make_eos(const cfd_config& c) {
     q.gp1 = q.g1 * q.p1;
     return q;
 }
+
+}  // namespace cfd
+
+namespace {
 
 void layout_sizes(const cfd_config& c, int& nv, int& g, int& pitch, long long& plane,
                   size_t& buf_elems) {
@@ -638,7 +644,7 @@ int cfd_last_error(char* buf, size_t len) {
 int cfd_nvar(int model) { return model == CFD_MODEL_ALLAIRE ? 6 : 4; }
 
 int cfd_device_bytes(const cfd_config* cfg, size_t* bytes) {
-    int r = validate(cfg);
+    int r = validate_config(cfg);
     if (r) return r;
     int nv, g, pitch;
     long long plane;
@@ -653,7 +659,7 @@ int cfd_device_bytes(const cfd_config* cfg, size_t* bytes) {
 int cfd_create(const cfd_config* cfg, cfd_solver** out) {
     if (!out) return fail(CFD_ERR_INVALID, "null output pointer");
     *out = nullptr;
-    int r = validate(cfg);
+    int r = validate_config(cfg);
     if (r) return r;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -1194,7 +1200,7 @@ int cfd_face_flux(const cfd_config* cfg, int nfaces, const double* stencils, dou
     if (c.dy <= 0) c.dy = 1;
     if (c.cfl <= 0) c.cfl = 0.5;
     c.precision = CFD_PREC_FP64;
-    int r = validate(&c);
+    int r = validate_config(&c);
     if (r) return r;
     if (nfaces <= 0) return CFD_OK;
     int nv = cfd_nvar(c.model);

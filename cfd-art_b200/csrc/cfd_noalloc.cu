@@ -1,10 +1,11 @@
 // A compute_dt entry point that allocates no device memory.
 //
-// Who needs it: code that runs where it may not call cudaMalloc -- inside a
-// CUDA graph being captured by someone else, in a real-time loop whose
-// memory is fixed up front, or inside a host application that owns every
-// device allocation through its own pool.  Such callers hand over the state
-// and a small output buffer they already own; the reduction's per-row scratch
+// Who needs it: callers that may not call cudaMalloc.  A host application or
+// framework that owns every device allocation through its own pool or a
+// fixed budget cannot let a library allocate behind its accounting, and a
+// latency-critical loop cannot afford the device-wide synchronisation that
+// cudaMalloc and cudaFree imply.  Such callers hand over the state and a
+// small output buffer they already own; the reduction's per-row scratch
 // lives in a fixed array compiled into this library instead.
 //
 // Scratch: g_noalloc_scratch, a file-scope __device__ array of
@@ -23,6 +24,7 @@
 #include <mutex>
 
 #include "../../include/cfdgpu.h"
+#include "cfd_config.h"
 #include "cfd_error.h"
 #include "cfd_sweep.cuh"
 
@@ -129,9 +131,9 @@ extern "C" {
 int cfd_compute_dt_noalloc(const cfd_config* cfg, const double* dev_state, int64_t plane,
                            int pitch, int n, double t, double* dev_out, void* stream) {
     if (!cfg || !dev_state || !dev_out) return cfd_fail(CFD_ERR_INVALID, "null argument");
-    if (cfg->model != CFD_MODEL_EULER && cfg->model != CFD_MODEL_ALLAIRE)
-        return cfd_fail(CFD_ERR_INVALID, "unknown model %d", cfg->model);
-    if (cfg->nx < 1 || cfg->ny < 1 || pitch < cfg->nx || plane < (int64_t)pitch * cfg->ny)
+    int r = validate_config(cfg);  // the checks cfd_create applies
+    if (r) return r;
+    if (pitch < cfg->nx || plane < (int64_t)pitch * cfg->ny)
         return cfd_fail(CFD_ERR_INVALID, "inconsistent grid %dx%d, pitch %d, plane %lld", cfg->nx,
                         cfg->ny, pitch, (long long)plane);
     if (cfg->ny > kNoAllocMaxRows)  // the fixed scratch holds one partial per grid row
@@ -147,7 +149,9 @@ int cfd_compute_dt_noalloc(const cfd_config* cfg, const double* dev_state, int64
     {
         // First call on a device: look up the device address of the scratch
         // array with that device current (the host-side symbol is only a
-        // stand-in).  Make this first call before any stream capture.
+        // stand-in), and load both models' kernels, so that no later call on
+        // this device loads code (which takes device memory) whichever model
+        // it is for.  Make this first call before any stream capture.
         std::lock_guard<std::mutex> lk(g_mu);
         if (!g_scratch_ptr[dev]) {
             void* p = nullptr;
@@ -155,6 +159,11 @@ int cfd_compute_dt_noalloc(const cfd_config* cfg, const double* dev_state, int64
             if (se != cudaSuccess || !p)
                 return cfd_fail(CFD_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s",
                                 cudaGetErrorString(se));
+            cudaFuncAttributes fa;
+            se = cudaFuncGetAttributes(&fa, noalloc_dt_kernel<MODEL_EULER>);
+            if (se == cudaSuccess) se = cudaFuncGetAttributes(&fa, noalloc_dt_kernel<MODEL_ALLAIRE>);
+            if (se != cudaSuccess)
+                return cfd_fail(CFD_ERR_CUDA, "loading the kernels: %s", cudaGetErrorString(se));
             g_scratch_ptr[dev] = static_cast<double*>(p);
         }
         scratch = g_scratch_ptr[dev];
@@ -175,13 +184,7 @@ int cfd_compute_dt_noalloc(const cfd_config* cfg, const double* dev_state, int64
     a.cfl = cfg->cfl;
     a.dx = cfg->dx;
     a.dy = cfg->dy;
-    a.eos.g1 = cfg->gamma1;
-    a.eos.p1 = cfg->pinf1;
-    a.eos.g2 = cfg->model == CFD_MODEL_ALLAIRE ? cfg->gamma2 : 1.4;
-    a.eos.p2 = cfg->model == CFD_MODEL_ALLAIRE ? cfg->pinf2 : 0.0;
-    a.eos.gm1_1 = a.eos.g1 - 1.0;
-    a.eos.gm1_2 = a.eos.g2 - 1.0;
-    a.eos.gp1 = a.eos.g1 * a.eos.p1;
+    a.eos = make_eos(*cfg);
     a.out = dev_out;
     a.scratch = scratch;
     if (cfg->model == CFD_MODEL_EULER)

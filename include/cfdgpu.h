@@ -221,9 +221,10 @@ int cfd_synchronize(cfd_solver* s);
 int cfd_state_device(cfd_solver* s, const void** dev_ptr, int64_t* plane, int* pitch);
 
 /* compute_dt without any device allocation, for callers that may not call
- * cudaMalloc (inside someone else's CUDA graph capture, in a real-time loop
- * with fixed memory, or in a host application that owns all device memory
- * through its own pool).  No counterpart in the reference: it is the
+ * cudaMalloc: a host application or framework that owns every device
+ * allocation through its own pool or a fixed budget, or a latency-critical
+ * loop that cannot take the device-wide synchronisation cudaMalloc and
+ * cudaFree imply.  No counterpart in the reference: it is the
  * reference's compute_dt (sourcecode/euler_timestep.cpp:7-44) computed on a
  * state the caller already holds on the device.
  *   dev_state: SoA FP64 planes (nvar planes `plane` elements apart, rows
@@ -236,8 +237,10 @@ int cfd_state_device(cfd_solver* s, const void** dev_ptr, int64_t* plane, int* p
  * that loads the library holds until exit; grids with more rows are rejected
  * with CFD_ERR_INVALID.  Every call shares that array and it keeps the last
  * call's contents, so calls that overlap on the GPU (concurrent streams or
- * threads) race: serialise them.  The first call on each device looks up the
- * array's device address with that device current; make that first call
+ * threads) race: serialise them.  The configuration is checked as
+ * cfd_create checks it (CFD_ERR_INVALID on a bad CFL, spacing or gamma).  The
+ * first call on each device looks up the array's device address with that
+ * device current and loads the kernels of both models; make that first call
  * before any stream capture.  Asynchronous on `stream` (NULL: the legacy
  * default stream); allocates nothing and frees nothing. */
 int cfd_compute_dt_noalloc(const cfd_config* cfg, const double* dev_state, int64_t plane,

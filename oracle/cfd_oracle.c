@@ -485,59 +485,70 @@ static void sweep_line(const eosp* q, const ref_params* p, const double* line, i
     }
 }
 
+/* The lines of a sweep are independent (each writes only its own cells of
+ * F and reads G), so they are split over OpenMP threads with per-thread
+ * line buffers; the results do not depend on the thread count. */
 static void x_sweep(const eosp* q, const ref_params* p, grid_t* G, grid_t* F, double dt) {
     int g = G->g, nx = G->nx, nv = G->nv;
-    double* out = malloc(sizeof(double) * nx * nv);
-    double* fl = malloc(sizeof(double) * (nx + 2 * g + 1) * nv);
-    double* us = calloc(nx + 2 * g + 1, sizeof(double));
-    double* zs = calloc(nx + 2 * g + 1, sizeof(double));
-    for (int i = g; i < G->ny + g; ++i) {
-        sweep_line(q, p, cell(G, i, 0), nx, g, dt, p->dx, p->dx, out, fl, us, zs);
-        for (int j = 0; j < nx; ++j) {
-            double* f = cell(F, i, j + g);
-            memcpy(f, out + (size_t)j * nv, sizeof(double) * nv);
-            if (q->model == ORACLE_EULER) euler_fixup(q, f, cell(G, i, j + g));
+#pragma omp parallel
+    {
+        double* out = malloc(sizeof(double) * nx * nv);
+        double* fl = malloc(sizeof(double) * (nx + 2 * g + 1) * nv);
+        double* us = calloc(nx + 2 * g + 1, sizeof(double));
+        double* zs = calloc(nx + 2 * g + 1, sizeof(double));
+#pragma omp for schedule(static)
+        for (int i = g; i < G->ny + g; ++i) {
+            sweep_line(q, p, cell(G, i, 0), nx, g, dt, p->dx, p->dx, out, fl, us, zs);
+            for (int j = 0; j < nx; ++j) {
+                double* f = cell(F, i, j + g);
+                memcpy(f, out + (size_t)j * nv, sizeof(double) * nv);
+                if (q->model == ORACLE_EULER) euler_fixup(q, f, cell(G, i, j + g));
+            }
         }
+        free(out);
+        free(fl);
+        free(us);
+        free(zs);
     }
-    free(out);
-    free(fl);
-    free(us);
-    free(zs);
 }
 
 static void y_sweep(const eosp* q, const ref_params* p, grid_t* G, grid_t* F, double dt) {
     int g = G->g, ny = G->ny, nv = G->nv;
     int a = q->model == ORACLE_EULER ? 1 : 2, b = a + 1;
     int len = ny + 2 * g;
-    double* line = malloc(sizeof(double) * len * nv);
-    double* out = malloc(sizeof(double) * ny * nv);
-    double* fl = malloc(sizeof(double) * (len + 1) * nv);
-    double* us = calloc(len + 1, sizeof(double));
-    double* zs = calloc(len + 1, sizeof(double));
     double h_flux = p->fix_dy_halfstep ? p->dy : p->dx; /* reference: params.dx */
-    for (int j = g; j < G->nx + g; ++j) {
-        for (int i = 0; i < len; ++i) {
-            double* L = line + (size_t)i * nv;
-            memcpy(L, cell(G, i, j), sizeof(double) * nv);
-            double t = L[a];
-            L[a] = L[b];
-            L[b] = -t;
+#pragma omp parallel
+    {
+        double* line = malloc(sizeof(double) * len * nv);
+        double* out = malloc(sizeof(double) * ny * nv);
+        double* fl = malloc(sizeof(double) * (len + 1) * nv);
+        double* us = calloc(len + 1, sizeof(double));
+        double* zs = calloc(len + 1, sizeof(double));
+#pragma omp for schedule(static)
+        for (int j = g; j < G->nx + g; ++j) {
+            for (int i = 0; i < len; ++i) {
+                double* L = line + (size_t)i * nv;
+                memcpy(L, cell(G, i, j), sizeof(double) * nv);
+                double t = L[a];
+                L[a] = L[b];
+                L[b] = -t;
+            }
+            sweep_line(q, p, line, ny, g, dt, h_flux, p->dy, out, fl, us, zs);
+            for (int i = 0; i < ny; ++i) {
+                double* f = cell(F, i + g, j);
+                memcpy(f, out + (size_t)i * nv, sizeof(double) * nv);
+                double t = f[a];
+                f[a] = -f[b];
+                f[b] = t;
+                if (q->model == ORACLE_EULER) euler_fixup(q, f, cell(G, i + g, j));
+            }
         }
-        sweep_line(q, p, line, ny, g, dt, h_flux, p->dy, out, fl, us, zs);
-        for (int i = 0; i < ny; ++i) {
-            double* f = cell(F, i + g, j);
-            memcpy(f, out + (size_t)i * nv, sizeof(double) * nv);
-            double t = f[a];
-            f[a] = -f[b];
-            f[b] = t;
-            if (q->model == ORACLE_EULER) euler_fixup(q, f, cell(G, i + g, j));
-        }
+        free(line);
+        free(out);
+        free(fl);
+        free(us);
+        free(zs);
     }
-    free(line);
-    free(out);
-    free(fl);
-    free(us);
-    free(zs);
 }
 
 static void swap_grids(grid_t* G, grid_t* F) {

@@ -32,6 +32,12 @@ double oracle_compute_dt(int model, const ref_params* p, const double* grid, int
 void oracle_face_flux(int model, const ref_params* p, const double* stencil, double dt, double dx,
                       double* flux, double* u_star, double* z_star);
 
+/* Initial ghosted grid and parameters of a seeded workload recipe
+ * (0 four-quadrant, 1 shock + bubbles, 2 water shock on an air bubble), equal
+ * bit for bit to the library's cfd_recipe_ic (oracle_recipes.c). */
+int oracle_recipe_ic(int recipe, int nx, int ny, unsigned long long seed, int nbubbles,
+                     double* grid, ref_params* p_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -196,6 +196,9 @@ def port_lib() -> C.CDLL:
     lib.oracle_face_flux.argtypes = [C.c_int, C.POINTER(RefParams), C.POINTER(C.c_double),
                                      C.c_double, C.c_double, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.oracle_recipe_ic.restype = C.c_int
+    lib.oracle_recipe_ic.argtypes = [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.c_int,
+                                     C.POINTER(C.c_double), C.POINTER(RefParams)]
     lib.oracle_compute_dt.restype = C.c_double
     lib.oracle_compute_dt.argtypes = [C.c_int, C.POINTER(RefParams), C.POINTER(C.c_double),
                                       C.c_int, C.c_double, C.POINTER(C.c_double)]
@@ -215,6 +218,24 @@ def port_run(model: str, p: RefParams, grid: np.ndarray, max_steps: int, n: int 
                            _dptr(future) if future is not None else None, int(max_steps),
                            C.byref(nn), C.byref(tt), _dptr(dt_log))
     return taken, nn.value, tt.value, dt_log[:taken]
+
+
+RECIPE = {"four_quadrant": 0, "shock_bubbles": 1, "water_shock_air_bubble": 2}
+
+
+def port_recipe_ic(recipe: str, nx: int, ny: int, seed: int = 20261203, nbubbles: int = 32):
+    """Seeded workload recipe built on the CPU side (oracle_recipes.c):
+    (ghosted AoS grid, RefParams, model name).  Equal bit for bit to the
+    library's host builder; the reference arm of bench.py uses it so that the
+    reference's loop runs without the library loaded."""
+    model = "allaire" if recipe == "water_shock_air_bubble" else "euler"
+    grid = np.zeros((ny + 4, nx + 4, nvar_of(model)))
+    p = RefParams()
+    r = port_lib().oracle_recipe_ic(RECIPE[recipe], int(nx), int(ny), int(seed), int(nbubbles),
+                                    _dptr(grid), C.byref(p))
+    if r:
+        raise ValueError(f"unknown recipe {recipe}")
+    return grid, p, model
 
 
 def port_face_flux(model: str, p: RefParams, stencil: np.ndarray, dt: float, dx: float):
@@ -298,6 +319,13 @@ def opcount_face(model: str, p: RefParams, stencil: np.ndarray, dt: float, dx: f
     return flux, us.value, (zs.value if model == "allaire" else None), _counts_dict(raw)["step"]
 
 
+def reference_dir() -> Path:
+    """The reference checkout: $CFD_REFERENCE_DIR, else a `reference`
+    directory beside the repository."""
+    env = os.environ.get("CFD_REFERENCE_DIR")
+    return Path(env) if env else HERE.parent.parent / "reference"
+
+
 def build(quiet: bool = True, ref: bool | None = None) -> None:
     """Build the oracles with oracle/Makefile (the reference part, and the
     reference's main loop linked with the GPU adapter, only where the
@@ -305,7 +333,7 @@ def build(quiet: bool = True, ref: bool | None = None) -> None:
     import subprocess
 
     targets = ["port", "opcount"]
-    ref_src = Path(os.environ.get("CFD_REFERENCE_DIR", "/root/reference"))
+    ref_src = reference_dir()
     if ref is None:
         ref = ref_src.exists()
     if ref:

@@ -9,6 +9,9 @@ import oracle_py as O
 
 ROOT = Path(__file__).resolve().parents[1]
 GOLDEN = ROOT / "tests" / "golden"
+# face known-answer fixtures of the reference build (make_golden.py)
+KATS = ["kat_faces_euler", "kat_faces_allaire", "kat_faces_euler_low_energy",
+        "kat_faces_allaire_low_energy"]
 
 
 def load_golden(name: str) -> dict:
@@ -70,3 +73,20 @@ def params_from_config(c, **over) -> O.RefParams:
     for k, v in over.items():
         setattr(p, k, v)
     return p, model
+
+
+def masschange_close(ours: str, ref: str) -> bool:
+    """Mass-change logs (E/sourcecode/euler_io.cpp:1219-1233) equal up to the
+    rounding of their sums: the reference sums serially, the GPU in a tree.
+    Times must be identical."""
+    a = [line.split() for line in ours.splitlines() if line.strip()]
+    b = [line.split() for line in ref.splitlines() if line.strip()]
+    if len(a) != len(b):
+        return False
+    for ra, rb in zip(a, b):
+        if ra[0] != rb[0] or len(ra) != len(rb):  # times are bit-identical
+            return False
+        for x, y in zip(map(float, ra[1:]), map(float, rb[1:])):
+            if abs(x - y) > max(1e-13, 1e-5 * abs(y)):
+                return False
+    return True

@@ -6,8 +6,9 @@
     python tests/golden/make_golden.py --out DIR  # everything, written under DIR instead
 
 Requires oracle/_ref/libref_{euler,allaire}.so (built by `make -C oracle ref`
-from the reference sources) and cfd-art_b200/lib/libcfdgpu.so (only for the
-host-side recipe initial conditions, which the reference does not have).
+from the reference sources) and oracle/_build/liboracle.so (the CPU-side
+builder of the seeded recipe initial conditions, which the reference does
+not have).
 Every fixture records the reference's own run: its set_ICs where the case is
 one of its test cases, its time loop, its flux solver.
 """
@@ -23,7 +24,6 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 OUT = HERE  # where fixtures are written (--out DIR: elsewhere, e.g. to compare)
 sys.path.insert(0, str(ROOT / "oracle"))
-sys.path.insert(0, str(ROOT / "cfd-art_b200"))
 
 import oracle_py as O  # noqa: E402
 
@@ -108,6 +108,65 @@ def kat_faces(model, nfaces, seed):
     print(f"kat_faces_{model}: {nfaces} faces")
 
 
+def kat_faces_low_energy(model, nfaces, seed):
+    """Adversarial known-answer faces for the physicality tests of MUSCL-
+    Hancock (E/headers/flux_solver_MUSCLhancock.hpp:178-189, 212-223): cells
+    whose specific internal energy is a tiny fraction r of their kinetic
+    energy (r log-uniform in [1e-15, 1e-10], i.e. on both sides of the
+    1e-13 relative margin below which the device defers to the reference's
+    exact recomputation), with fast flow, so that the extrapolated and
+    evolved face states sit at e ~ 0 and the reference's zero-slope and
+    first-order fallbacks fire on some faces and not on others.  Stencils
+    whose cells fail the reference's own input assert, or whose flux is not
+    finite, are dropped."""
+    rng = np.random.default_rng(seed)
+    n = 4 * nfaces
+    r = 10.0 ** rng.uniform(-15, -10, (n, 4))
+    if model == "euler":
+        p = O.make_params(2, 2, 1.0, 1.0, 1.4, limiter="minmod")
+        rho = rng.lognormal(0, 1, (n, 4))
+        u = rng.normal(0, 20, (n, 4))
+        v = rng.normal(0, 20, (n, 4))
+        ke = 0.5 * (u * u + v * v)
+        e = r * ke
+        U = np.stack([rho, rho * u, rho * v, rho * e + rho * ke], -1)
+        ru = U[..., 0]
+        e_chk = U[..., 3] / ru - 0.5 * ((U[..., 1] / ru) ** 2 + (U[..., 2] / ru) ** 2)
+    else:
+        # air only (z = 0): with any stiffened-gas share a state this close
+        # to e = 0 has a negative squared sound speed (p -> -k), and its flux
+        # is NaN in the reference
+        p = O.make_params(2, 2, 1.0, 1.0, 4.4, 6e8, 1.4, 0.0, limiter="minmod")
+        z = np.zeros((n, 4))
+        r1 = rng.uniform(900, 1100, (n, 4))
+        r2 = rng.uniform(0.5, 2, (n, 4))
+        u = rng.normal(0, 300, (n, 4))
+        v = rng.normal(0, 300, (n, 4))
+        ke = 0.5 * (u * u + v * v)
+        rho = z * r1 + (1 - z) * r2
+        e = r * ke
+        U = np.stack([z * r1, (1 - z) * r2, rho * u, rho * v, rho * e + rho * ke, z], -1)
+        ru = U[..., 0] + U[..., 1]
+        e_chk = U[..., 4] / ru - 0.5 * ((U[..., 2] / ru) ** 2 + (U[..., 3] / ru) ** 2)
+    U = U[(e_chk >= 0.0).all(axis=1)]
+    dt, dx = (1e-3, 1e-2) if model == "euler" else (1e-6, 1e-2)
+    rows = []
+    for f in range(len(U)):
+        fl, a, b = O.ref_face_flux(model, p, U[f], dt, dx)
+        if np.isfinite(fl).all() and np.isfinite(a):  # known answers, not NaN
+            rows.append((U[f], fl, a, b if b is not None else 0.0))
+        if len(rows) == nfaces:
+            break
+    U = np.ascontiguousarray(np.stack([r[0] for r in rows]))
+    F = np.stack([r[1] for r in rows])
+    us = np.array([r[2] for r in rows])
+    zs = np.array([r[3] for r in rows])
+    np.savez_compressed(OUT / f"kat_faces_{model}_low_energy.npz", stencils=U, flux=F,
+                        u_star=us, z_star=zs, dt=np.array(dt), dx=np.array(dx),
+                        **{"p_" + k: np.array(v) for k, v in params_dict(p).items()})
+    print(f"kat_faces_{model}_low_energy: {len(U)} faces")
+
+
 def main():
     assert O.ref_available("euler") and O.ref_available("allaire"), "build oracle/_ref first"
     # reference test cases through the reference's own set_ICs and time loop
@@ -121,19 +180,18 @@ def main():
          *case_run("allaire", "ST1_y", 12, 80, 60, limiter="mc"))
 
     # four-quadrant Riemann problem, 200x200 to t = 0.3 (van Leer, CFL 0.8):
-    # the recipe IC is built by the library's host hook, stepped by the reference
-    import cfdgpu as G
-    cfg = G.recipe_config("four_quadrant", 200, 200)
-    ic = G.recipe_ic(cfg, "four_quadrant")
-    p = O.make_params(200, 200, cfg.dx, cfg.dy, 1.4, limiter="vanleer", cfl=0.8, T=0.3)
+    # the recipe IC is built by the CPU-side recipe builder
+    # (oracle/oracle_recipes.c, bit-identical to the library's host hook),
+    # stepped by the reference
+    ic, pr, _ = O.port_recipe_ic("four_quadrant", 200, 200)
+    p = O.make_params(200, 200, pr.dx, pr.dy, 1.4, limiter="vanleer", cfl=0.8, T=0.3)
     grid = ic.copy()
     taken, n, t, dts = O.ref_run("euler", p, grid, 100000)
     save("euler_four_quadrant_200x200", "euler", ic, grid, p, taken, n, t, dts, store_full=False)
 
     # water shock on an air bubble (PVRS wave speeds, z clipped to [1e-6, 1-1e-6])
-    cfg = G.recipe_config("water_shock_air_bubble", 64, 32)
-    ic = G.recipe_ic(cfg, "water_shock_air_bubble")
-    p = O.make_params(64, 32, cfg.dx, cfg.dy, 4.4, 6e8, 1.4, 0.0, cfl=0.6, wavespeed="pvrs",
+    ic, pr, _ = O.port_recipe_ic("water_shock_air_bubble", 64, 32)
+    p = O.make_params(64, 32, pr.dx, pr.dy, 4.4, 6e8, 1.4, 0.0, cfl=0.6, wavespeed="pvrs",
                       z_min=1e-6)
     grid = ic.copy()
     taken, n, t, dts = O.ref_run("allaire", p, grid, 40)
@@ -141,6 +199,20 @@ def main():
 
     kat_faces("euler", 256, 1)
     kat_faces("allaire", 256, 2)
+    kat_faces_low_energy("euler", 1024, 3)
+    kat_faces_low_energy("allaire", 1024, 4)
+
+    # long horizons at the benchmarked configurations' step counts on reduced
+    # grids: shock + bubbles (Euler, 2000 steps at CFL 0.8) and the water
+    # shock on an air bubble (Allaire, PVRS speeds, alpha clip, 1500 steps at
+    # CFL 0.6), from the CPU-side recipe builder (oracle/oracle_recipes.c)
+    for recipe, model, nx, ny, nb, steps in (("shock_bubbles", "euler", 64, 64, 8, 2000),
+                                             ("water_shock_air_bubble", "allaire", 64, 32, 1,
+                                              1500)):
+        ic, p, _ = O.port_recipe_ic(recipe, nx, ny, 20261203, nb)
+        grid = ic.copy()
+        taken, n, t, dts = O.ref_run(model, p, grid, steps)
+        save(f"{model}_{recipe}_{nx}x{ny}_{steps}steps", model, ic, grid, p, taken, n, t, dts)
 
     for name, model, settings in OUTPUT_RUNS:
         output_run(name, model, settings)

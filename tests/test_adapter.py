@@ -8,14 +8,15 @@ stub whose device calls the CPU oracle answers (ref_main_stub_*,
 tests/adapter/device_stub.cpp).  The stub build must write every output file
 of the reference's own run byte for byte -- which checks the adapter's call
 sequence (which call takes the step, when the state is read back, where the
-masses go) -- and the library build must fail loudly where no GPU exists.
+masses go); the library build must write them on a GPU (the mass-change log
+to the rounding of its sums) and fail loudly where no GPU exists.
 """
 import os
 import subprocess
 
 import pytest
 
-from cfdtest import GOLDEN, ROOT, load_golden
+from cfdtest import GOLDEN, ROOT, load_golden, masschange_close
 
 REF = ROOT / "oracle" / "_ref"
 RUNS = sorted(p.stem for p in GOLDEN.glob("outputs_*.npz")) + \
@@ -74,3 +75,23 @@ def test_adapter_on_library_fails_loudly_without_device(model, tmp_path):
     assert r.returncode == 1
     assert "cfd_create failed (-2)" in r.stderr
     assert files == {}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("run", RUNS)
+def test_adapter_on_library_writes_reference_outputs(run, tmp_path):
+    """The reference's unmodified main loop (E/sourcecode/main.cpp:17-49,
+    E/headers/simulation.hpp:36-67) driving GpuProblem on the device: every
+    output file of the reference's own run, states, schlieren frames and
+    lineouts byte for byte, the mass-change log to the rounding of its sums
+    (the reference sums serially, the device in a tree)."""
+    fx = load_golden(run)
+    r, files = _run(REF / f"ref_main_gpu_{_model(run)}", fx, tmp_path)
+    assert r.returncode == 0, r.stderr[-2000:]
+    expected = {k: bytes(v) for k, v in fx.items() if k != "settings"}
+    assert sorted(files) == sorted(expected)
+    for name, data in expected.items():
+        if name.endswith("-masschange.dat"):
+            assert masschange_close(files[name].decode(), data.decode()), name
+        else:
+            assert files[name] == data, name

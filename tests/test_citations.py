@@ -13,7 +13,7 @@ import pytest
 
 from cfdtest import ROOT
 
-REF = Path(os.environ.get("CFD_REFERENCE_DIR", "/root/reference"))
+REF = Path(os.environ.get("CFD_REFERENCE_DIR") or ROOT.parent / "reference")
 CITE = re.compile(r"([A-Za-z_0-9]+\.(?:hpp|cpp)):(\d+)(?:-(\d+))?")
 DECL = re.compile(r"^(?:int|double|void|const char\*|size_t)\s+(cfd_[a-z_0-9]+)\s*\(")
 

@@ -10,25 +10,11 @@ import subprocess
 import numpy as np
 import pytest
 
-from cfdtest import GOLDEN, ROOT
+from cfdtest import GOLDEN, ROOT, masschange_close
 
 pytestmark = pytest.mark.gpu
 DRIVER = ROOT / "cfd-art_b200" / "lib" / "run-cfd-simulation"
 RUNS = sorted(p.stem for p in GOLDEN.glob("outputs_*.npz"))
-
-
-def _masschange_close(ours: str, ref: str) -> bool:
-    a = [line.split() for line in ours.splitlines() if line.strip()]
-    b = [line.split() for line in ref.splitlines() if line.strip()]
-    if len(a) != len(b):
-        return False
-    for ra, rb in zip(a, b):
-        if ra[0] != rb[0] or len(ra) != len(rb):  # times are bit-identical
-            return False
-        for x, y in zip(map(float, ra[1:]), map(float, rb[1:])):
-            if abs(x - y) > max(1e-13, 1e-5 * abs(y)):
-                return False
-    return True
 
 
 @pytest.mark.parametrize("run", RUNS)
@@ -46,6 +32,6 @@ def test_driver_outputs_match_reference(tmp_path, run):
     for name, ref in fx.items():
         data = (out / name).read_bytes()
         if name.endswith("-masschange.dat"):
-            assert _masschange_close(data.decode(), ref.tobytes().decode()), name
+            assert masschange_close(data.decode(), ref.tobytes().decode()), name
         else:
             assert data == ref.tobytes(), name

@@ -63,6 +63,26 @@ def test_mixed_vs_fp64(recipe, nx, ny, steps):
     assert l1 <= TOL_MIXED_L1
 
 
+@pytest.mark.parametrize("recipe,nx,ny,nb,steps", [
+    ("shock_bubbles", 4096, 4096, 32, 2000),
+    ("water_shock_air_bubble", 2048, 1024, 1, 1500),
+])
+def test_mixed_vs_fp64_at_benchmarked_configs(recipe, nx, ny, nb, steps):
+    """The mixed form against the plain FP64 form (bit-identical to the
+    reference) at the benchmarked grids over their full stated step counts."""
+    cfg = G.recipe_config(recipe, nx, ny)
+    ic = G.recipe_ic(cfg, recipe, nbubbles=nb)
+    ref, sr = _fp64_run(cfg, ic, steps)
+    out, sm = _mixed_run(cfg, ic, steps)
+    assert sm.n == sr.n == steps
+    model = "euler" if cfg.model == G.EULER else "allaire"
+    l1, linf = _errors(out, ref, model)
+    print(f"{recipe} {nx}x{ny} {steps} steps: mixed vs FP64 L1 {l1:.2e} Linf {linf:.2e}, "
+          f"t {sm.t:.9g} vs {sr.t:.9g}")
+    assert np.isfinite(out).all()
+    assert l1 <= TOL_MIXED_L1
+
+
 @pytest.mark.parametrize("case,nx,ny", [("ST2_x", 200, 20), ("cross", 96, 80),
                                         ("shocked_helium_bubble", 130, 36)])
 def test_mixed_reference_cases(case, nx, ny):

@@ -11,7 +11,7 @@ import pytest
 
 import cfdgpu as G
 import oracle_py as O
-from cfdtest import (GOLDEN, config_from_params, density, ghost_grid, load_golden, params_from,
+from cfdtest import (GOLDEN, KATS, config_from_params, density, ghost_grid, load_golden, params_from,
                      params_from_config, rel_l1)
 
 pytestmark = pytest.mark.gpu
@@ -20,9 +20,14 @@ TOL_L1 = 1e-12  # relative L1 density error bound of the plain FP64 form
 FIXTURES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("kat_", "outputs_")))
 
 
-@pytest.mark.parametrize("model", ["euler", "allaire"])
-def test_device_faces_match_reference_kat(model):
-    fx = load_golden(f"kat_faces_{model}")
+@pytest.mark.parametrize("name", KATS)
+def test_device_faces_match_reference_kat(name):
+    """Face KATs of the reference build, including the low-energy ones whose
+    face states straddle the margin of the physicality shortcut
+    (is_physical_from_prim): the device's fallback decisions must be the
+    reference's, or the fluxes would differ."""
+    model = name.split("_")[2]
+    fx = load_golden(name)
     p = params_from(fx)
     cfg = config_from_params(p, model)
     flux, us, zs = G.face_flux(cfg, fx["stencils"], float(fx["dt"]), float(fx["dx"]))
@@ -169,6 +174,27 @@ def test_recipe_shock_bubbles_512_matches_oracle():
     out, n, t, st = _gpu_run(cfg, ic, 6, host_loop=False)
     assert n == 6
     assert np.array_equal(out[2:-2, 2:-2], ref[2:-2, 2:-2])
+
+
+@pytest.mark.parametrize("recipe,nx,ny,nb,steps", [
+    ("shock_bubbles", 4096, 4096, 32, 10),           # BASELINE config 2's grid
+    ("water_shock_air_bubble", 2048, 1024, 1, 10),   # BASELINE config 3's grid
+])
+def test_full_size_grid_matches_oracle(recipe, nx, ny, nb, steps):
+    """The benchmarked grids at full size against the oracle (the plain-C
+    restatement, pinned bit for bit to the reference build), over the first
+    steps of their stated runs (the reference's time loop,
+    E/headers/simulation.hpp:48-61): every cell, step count and time equal."""
+    ic, p, model = O.port_recipe_ic(recipe, nx, ny, 20261203, nb)
+    cfg = config_from_params(p, model)
+    ref = ic.copy()
+    taken, n_ref, t_ref, _ = O.port_run(model, p, ref, steps)
+    assert taken == steps
+    out, n, t, st = _gpu_run(cfg, ic, steps, host_loop=False)
+    assert (n, t) == (n_ref, t_ref)
+    fin, want = out[2:-2, 2:-2], ref[2:-2, 2:-2]
+    assert rel_l1(density(fin, model), density(want, model)) <= TOL_L1
+    assert np.array_equal(fin, want)
 
 
 def test_large_grid_device_loop_equals_host_loop():

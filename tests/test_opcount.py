@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle_py as O
-from cfdtest import GOLDEN, ghost_grid, load_golden, params_from
+from cfdtest import GOLDEN, KATS, ghost_grid, load_golden, params_from
 
 pytestmark = pytest.mark.skipif(not (O.PORT_DIR / "libopcount.so").exists(),
                                 reason="oracle/_build/libopcount.so not built")
@@ -35,9 +35,10 @@ def test_counted_run_reproduces_golden_run(name):
     assert counts["step"]["div"] > 0 and counts["dt"]["sqrt"] == p.nx * p.ny * taken
 
 
-@pytest.mark.parametrize("model", ["euler", "allaire"])
-def test_counted_faces_reproduce_reference_kats(model):
-    fx = load_golden(f"kat_faces_{model}")
+@pytest.mark.parametrize("name", KATS)
+def test_counted_faces_reproduce_reference_kats(name):
+    model = name.split("_")[2]
+    fx = load_golden(name)
     p = params_from(fx)
     dt, dx = float(fx["dt"]), float(fx["dx"])
     for f in range(fx["stencils"].shape[0]):

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle_py as O
-from cfdtest import GOLDEN, density, ghost_grid, load_golden, params_from, rel_l1
+from cfdtest import GOLDEN, KATS, density, ghost_grid, load_golden, params_from, rel_l1
 
 FIXTURES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("kat_", "outputs_")))
 
@@ -34,9 +34,10 @@ def test_port_reproduces_golden_run(name):
     assert rel_l1(density(fin, model), fx["rho"]) <= 1e-12
 
 
-@pytest.mark.parametrize("model", ["euler", "allaire"])
-def test_port_reproduces_reference_faces(model):
-    fx = load_golden(f"kat_faces_{model}")
+@pytest.mark.parametrize("name", KATS)
+def test_port_reproduces_reference_faces(name):
+    model = name.split("_")[2]
+    fx = load_golden(name)
     p = params_from(fx)
     dt, dx = float(fx["dt"]), float(fx["dx"])
     for f in range(fx["stencils"].shape[0]):
@@ -140,3 +141,26 @@ def test_port_and_writers_reproduce_reference_final_outputs(tmp_path, run):
         name = prefix + suffix
         assert name in fx, name
         assert (tmp_path / name).read_bytes() == fx[name].tobytes(), name
+
+
+@pytest.mark.parametrize("recipe,nx,ny,nb,seed", [
+    ("four_quadrant", 64, 48, 0, 0),
+    ("shock_bubbles", 300, 200, 32, 5),
+    ("shock_bubbles", 97, 131, 4, 20261203),
+    ("water_shock_air_bubble", 200, 100, 1, 7),
+    ("water_shock_air_bubble", 64, 32, 1, 20261203),
+])
+def test_port_recipes_equal_library_builder(recipe, nx, ny, nb, seed):
+    """The CPU-side recipe builder that bench.py's reference arm uses (so that
+    the reference runs without the library loaded) gives the library host
+    builder's grid and parameters bit for bit."""
+    import cfdgpu as G
+
+    grid, p, _model = O.port_recipe_ic(recipe, nx, ny, seed, nb)
+    cfg = G.recipe_config(recipe, nx, ny)
+    ic = G.recipe_ic(cfg, recipe, seed=seed, nbubbles=nb)
+    assert np.array_equal(grid, ic) and np.array_equal(np.signbit(grid), np.signbit(ic))
+    assert (p.dx, p.dy, p.cfl, p.limiter, p.wavespeed, p.z_min, p.gamma1, p.pinf1, p.gamma2,
+            p.pinf2) == (cfg.dx, cfg.dy, cfg.cfl, cfg.limiter, cfg.wavespeed, cfg.z_min,
+                         cfg.gamma1, cfg.pinf1, cfg.gamma2, cfg.pinf2)
+    assert tuple(p.bc) == tuple(cfg.bc) and (p.T == cfg.T or (np.isinf(p.T) and np.isinf(cfg.T)))
