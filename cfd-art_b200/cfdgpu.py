@@ -20,7 +20,7 @@ PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "lib" / "libcfdgpu.so"
 
 EULER, ALLAIRE = 0, 1
-FP64, MIXED = 0, 1
+FP64, MIXED, FP64_FAST = 0, 1, 2  # CFD_PREC_*
 TRANSMISSIVE, REFLECTIVE = 0, 1
 LIMITERS = {"minmod": 0, "vanleer": 1, "mc": 2, "unlimited": 3}
 FLUX = {"MUSCL": 0, "Godunov": 1}

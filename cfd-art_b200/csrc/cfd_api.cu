@@ -132,12 +132,13 @@ int validate_config(const cfd_config* c) {
     if (!c) return fail(CFD_ERR_INVALID, "null config");
     if (c->model != CFD_MODEL_EULER && c->model != CFD_MODEL_ALLAIRE)
         return fail(CFD_ERR_INVALID, "unknown model %d", c->model);
-    if (c->precision != CFD_PREC_FP64 && c->precision != CFD_PREC_MIXED)
+    if (c->precision != CFD_PREC_FP64 && c->precision != CFD_PREC_MIXED &&
+        c->precision != CFD_PREC_FP64_FAST)
         return fail(CFD_ERR_INVALID, "unknown precision %d", c->precision);
-    if (c->precision == CFD_PREC_MIXED)
+    if (c->precision != CFD_PREC_FP64)
         return fail(CFD_ERR_UNSUPPORTED,
-                    "a single solver is FP64; mixed precision runs as a batch member "
-                    "(cfd_batch_add) or through the server");
+                    "a single solver is the bit-identical FP64 form; the mixed and fast FP64 "
+                    "forms run as batch members (cfd_batch_add) or through the server");
     if (c->nx < 2 || c->ny < 2)
         return fail(CFD_ERR_INVALID, "grid %dx%d: need at least 2 cells per direction", c->nx,
                     c->ny);
@@ -836,8 +837,6 @@ int cfd_upload_case(cfd_solver* s, const char* test_case, uint64_t seed, int n, 
     std::vector<cfdic::Op> ops;
     cfdic::Eos q;
     int r = cfdic::case_program(&s->cfg, test_case, seed, ops, q);
-    if (r == CFD_ERR_UNSUPPORTED)
-        return fail(r, "test case %s is built on the host only (cfd_case_ic)", test_case);
     if (r) return fail(r, "unknown test case %s", test_case);
     return upload_program(s, ops, q, n, t);
 }

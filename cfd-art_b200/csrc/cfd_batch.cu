@@ -11,8 +11,10 @@
 // against a device-memory budget, so a server can keep adding work while
 // others run.
 //
-// Precision: the mixed form (FP32 + compensation word state; see
-// cfd_mixed.cuh).  The plain FP64 form uses cfd_solver (cfd_api.cu).
+// Precision, per member: the mixed form (FP32 + compensation word state;
+// cfd_mixed.cuh) or the fast FP64 form (cfd_fast64.cuh), which stores FP64
+// values in the same planes; each (model, form) pair has its own tile lists
+// and launches.  The bit-identical FP64 form uses cfd_solver (cfd_api.cu).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,6 +30,7 @@
 #include "../../include/cfdgpu.h"
 #include "cfd_checkpoint.h"
 #include "cfd_error.h"
+#include "cfd_fast64.cuh"
 #include "cfd_ic.h"
 #include "cfd_march.cuh"
 #include "cfd_mixed.cuh"
@@ -126,6 +129,38 @@ int launch_segment(const MixedArgs& a, int sms, cudaStream_t st) {
     return CFD_OK;
 }
 
+// The fast FP64 form's sweeps (cfd_fast64.cuh), launched like the mixed
+// warp forms: x by warp segments, y by marching strips.
+template <int MODEL>
+int march64_per_sm() {
+    static int per_sm = 0;
+    if (!per_sm) {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, fast::fast_march_kernel<MODEL>, 128, 0);
+        if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    }
+    return per_sm;
+}
+
+template <int MODEL>
+int launch_fast(int dir, const MixedArgs& a, int sms, cudaStream_t st) {
+    static int seg_per_sm = 0;
+    if (dir == DIR_X && !seg_per_sm) {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &seg_per_sm, fast::fast_segment_x_kernel<MODEL>, 128, 0);
+        if (e != cudaSuccess || seg_per_sm < 1) seg_per_sm = 1;
+    }
+    const int per_sm = dir == DIR_X ? seg_per_sm : march64_per_sm<MODEL>();
+    const int warps = std::max(1, std::min(a.ntiles, per_sm * sms * 4));
+    if (dir == DIR_X)
+        fast::fast_segment_x_kernel<MODEL><<<(warps + 3) / 4, 128, 0, st>>>(a);
+    else
+        fast::fast_march_kernel<MODEL><<<(warps + 3) / 4, 128, 0, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "fast FP64 sweep launch: %s", cudaGetErrorString(e));
+    return CFD_OK;
+}
+
 template <int MODEL>
 int launch_shape(int dir, int shape, const MixedArgs& a, int grid, cudaStream_t st) {
     if (dir == DIR_X) return launch_segment<MODEL>(a, grid, st);
@@ -165,8 +200,30 @@ int march_rows(const std::vector<std::pair<int, int>>& grids, long long slots) {
 
 // ---- conversion kernels ----------------------------------------------------
 
-// Ghosted FP64 AoS grid -> packed value/compensation planes, plus an FP64
-// SoA copy for the initial wave-speed reduction.
+// One cell of an FP64 member's packed planes (the storage of cfd_fast64.cuh).
+__device__ __forceinline__ void store_packed64(const Inst& I, int buf, long long o, const double* U) {
+    reinterpret_cast<double2*>(I.q4[buf][0])[o] = make_double2(U[0], U[1]);
+    reinterpret_cast<double2*>(I.q4[buf][1])[o] = make_double2(U[2], U[3]);
+    if (I.nv == 6) {
+        reinterpret_cast<double*>(I.q2[buf][0])[o] = U[4];
+        reinterpret_cast<double*>(I.q2[buf][1])[o] = U[5];
+    }
+}
+__device__ __forceinline__ void load_packed64(const Inst& I, int buf, long long o, double* U) {
+    const double2 a = reinterpret_cast<const double2*>(I.q4[buf][0])[o];
+    const double2 b = reinterpret_cast<const double2*>(I.q4[buf][1])[o];
+    U[0] = a.x;
+    U[1] = a.y;
+    U[2] = b.x;
+    U[3] = b.y;
+    if (I.nv == 6) {
+        U[4] = reinterpret_cast<const double*>(I.q2[buf][0])[o];
+        U[5] = reinterpret_cast<const double*>(I.q2[buf][1])[o];
+    }
+}
+
+// Ghosted FP64 AoS grid -> packed planes (value/compensation, or FP64), plus
+// an FP64 SoA copy for the initial wave-speed reduction.
 __global__ void ghosted_to_mixed(const double* __restrict__ src, Inst I,
                                  double* __restrict__ soa, int g) {
     long long n = (long long)I.nx * I.ny;
@@ -176,6 +233,12 @@ __global__ void ghosted_to_mixed(const double* __restrict__ src, Inst I,
         int i = (int)(idx / I.nx), j = (int)(idx % I.nx);
         const double* c = src + ((long long)(i + g) * (I.nx + 2 * g) + (j + g)) * nv;
         long long o = (long long)i * I.pitch + j;
+        if (I.fp64) {
+            double U[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            for (int k = 0; k < nv; ++k) soa[k * I.plane + o] = U[k] = c[k];
+            store_packed64(I, 0, o, U);
+            continue;
+        }
         float h[6], l[6];
         for (int k = 0; k < nv; ++k) {
             double x = c[k];
@@ -192,8 +255,8 @@ __global__ void ghosted_to_mixed(const double* __restrict__ src, Inst I,
     }
 }
 
-// FP64 SoA planes (the instance's pitch and plane) -> packed value /
-// compensation planes of buffer 0.
+// FP64 SoA planes (the instance's pitch and plane) -> packed planes of
+// buffer 0.
 __global__ void soa_to_mixed(const double* __restrict__ soa, Inst I) {
     long long n = (long long)I.nx * I.ny;
     const int nv = I.nv;
@@ -201,6 +264,12 @@ __global__ void soa_to_mixed(const double* __restrict__ soa, Inst I) {
          idx += (long long)gridDim.x * blockDim.x) {
         int i = (int)(idx / I.nx), j = (int)(idx % I.nx);
         long long o = (long long)i * I.pitch + j;
+        if (I.fp64) {
+            double U[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            for (int k = 0; k < nv; ++k) U[k] = soa[k * I.plane + o];
+            store_packed64(I, 0, o, U);
+            continue;
+        }
         float h[6], l[6];
         for (int k = 0; k < nv; ++k) {
             double x = soa[k * I.plane + o];
@@ -218,6 +287,7 @@ __global__ void soa_to_mixed(const double* __restrict__ soa, Inst I) {
 
 // Packed planes of buffer `buf` (< 0: the current one) -> FP64 AoS with the
 // boundary mirror in the ghost strips (g = 0: interior only); corners are zero.
+// Mixed members give value + compensation, FP64 members their values.
 __global__ void mixed_to_ghosted(Inst I, int buf, double* __restrict__ dst, int g, int im,
                                  int it, int use_bc) {
     if (buf < 0) buf = I.st->cur & 1;  // the current buffer
@@ -240,13 +310,20 @@ __global__ void mixed_to_ghosted(Inst I, int buf, double* __restrict__ dst, int 
         if (i < 0) { si = -i - 1; if (use_bc && I.bc[2]) neg = it; }
         else if (i >= ny) { si = 2 * ny - 1 - i; if (use_bc && I.bc[3]) neg = it; }
         long long o = (long long)si * I.pitch + sj;
-        float4 a = I.q4[buf][0][o], b = I.q4[buf][1][o];
-        double v[6] = {(double)a.x + b.x, (double)a.y + b.y, (double)a.z + b.z, (double)a.w + b.w,
-                       0.0, 0.0};
-        if (nv == 6) {
-            float2 c = I.q2[buf][0][o], e = I.q2[buf][1][o];
-            v[4] = (double)c.x + e.x;
-            v[5] = (double)c.y + e.y;
+        double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (I.fp64) {
+            load_packed64(I, buf, o, v);
+        } else {
+            float4 a = I.q4[buf][0][o], b = I.q4[buf][1][o];
+            v[0] = (double)a.x + b.x;
+            v[1] = (double)a.y + b.y;
+            v[2] = (double)a.z + b.z;
+            v[3] = (double)a.w + b.w;
+            if (nv == 6) {
+                float2 c = I.q2[buf][0][o], e = I.q2[buf][1][o];
+                v[4] = (double)c.x + e.x;
+                v[5] = (double)c.y + e.y;
+            }
         }
         for (int k = 0; k < nv; ++k) d[k] = (k == neg) ? -v[k] : v[k];
     }
@@ -360,7 +437,7 @@ struct cfd_batch {
     TileEnt* d_tiles = nullptr;
     size_t d_tiles_cap = 0;
     struct Group {
-        int model, dir, shape, ntiles, offset;
+        int model, fp64, dir, shape, ntiles, offset;
         int rows;  // marching strips: cells along the sweep per strip
     };
     std::vector<Group> groups;
@@ -369,7 +446,8 @@ struct cfd_batch {
     // both models, and the strips adapt to the members)
     int shape[2][2] = {{0, kMarchShape}, {0, kMarchShape}};
     int march_fixed[2] = {0, 0};  // strip length set by the caller (0: chosen per tile list)
-    int march_used[2] = {0, 0};   // strip length of the current tile list
+    int march_used[2] = {0, 0};   // strip length of the current mixed tile list
+    int march_used64[2] = {0, 0}; // strip length of the current fast FP64 tile list
     int sms = 148;
     // graph of `graph_steps` ticks for the current membership
     cudaGraphExec_t graph = nullptr;
@@ -410,29 +488,38 @@ int build_tables(cfd_batch* b) {
     if (int r = wait_uploads(b)) return r;
     if (!b->dirty) return CFD_OK;
     b->groups.clear();
-    // the y shape of each model, with the strip length of a marching sweep
-    Shape shape_y[2];
-    for (int model = 0; model < 2; ++model) {
-        shape_y[model] = kShapesY[b->shape[model][DIR_Y]];
-        b->march_used[model] = 0;
-        if (b->shape[model][DIR_Y] != kMarchShape) continue;
-        std::vector<std::pair<int, int>> grids;
-        for (const Member& m : b->members)
-            if (m.cfg.model == model && !m.final) grids.emplace_back(m.cfg.nx, m.cfg.ny);
-        if (grids.empty()) continue;
-        const int per_sm = model == CFD_MODEL_EULER ? march_per_sm<MODEL_EULER, DIR_Y>()
-                                                    : march_per_sm<MODEL_ALLAIRE, DIR_Y>();
-        shape_y[model].ts = b->march_fixed[model]
-                                ? b->march_fixed[model]
-                                : march_rows(grids, (long long)per_sm * b->sms * 4);
-        b->march_used[model] = shape_y[model].ts;
-    }
+    // the y shape of each (model, form), with the strip length of a marching
+    // sweep; the fast FP64 form always marches in y
+    Shape shape_y[2][2];
+    for (int model = 0; model < 2; ++model)
+        for (int f64 = 0; f64 < 2; ++f64) {
+            const int shp = f64 ? kMarchShape : b->shape[model][DIR_Y];
+            shape_y[model][f64] = kShapesY[shp];
+            int& used = f64 ? b->march_used64[model] : b->march_used[model];
+            used = 0;
+            if (shp != kMarchShape) continue;
+            std::vector<std::pair<int, int>> grids;
+            for (const Member& m : b->members)
+                if (m.cfg.model == model && m.inst.fp64 == f64 && !m.final)
+                    grids.emplace_back(m.cfg.nx, m.cfg.ny);
+            if (grids.empty()) continue;
+            const int per_sm =
+                f64 ? (model == CFD_MODEL_EULER ? march64_per_sm<MODEL_EULER>()
+                                                : march64_per_sm<MODEL_ALLAIRE>())
+                    : (model == CFD_MODEL_EULER ? march_per_sm<MODEL_EULER, DIR_Y>()
+                                                : march_per_sm<MODEL_ALLAIRE, DIR_Y>());
+            shape_y[model][f64].ts = b->march_fixed[model]
+                                         ? b->march_fixed[model]
+                                         : march_rows(grids, (long long)per_sm * b->sms * 4);
+            used = shape_y[model][f64].ts;
+        }
     std::vector<Inst> insts(b->members.size());
     for (size_t i = 0; i < b->members.size(); ++i) {
         Member& m = b->members[i];
         int model = m.cfg.model;
-        m.inst.tiles_x = tiles_for(m.cfg.nx, m.cfg.ny, DIR_X, kShapesX[b->shape[model][DIR_X]]);
-        m.inst.tiles_y = tiles_for(m.cfg.nx, m.cfg.ny, DIR_Y, shape_y[model]);
+        const int shx = m.inst.fp64 ? 0 : b->shape[model][DIR_X];
+        m.inst.tiles_x = tiles_for(m.cfg.nx, m.cfg.ny, DIR_X, kShapesX[shx]);
+        m.inst.tiles_y = tiles_for(m.cfg.nx, m.cfg.ny, DIR_Y, shape_y[model][m.inst.fp64]);
         insts[i] = m.inst;
     }
     // largest instances first within each group so the tail of a sweep is
@@ -445,37 +532,40 @@ int build_tables(cfd_batch* b) {
     });
     std::vector<TileEnt> all;
     for (int model = 0; model < 2; ++model)
-        for (int dir = 0; dir < 2; ++dir) {
-            cfd_batch::Group g;
-            g.model = model;
-            g.dir = dir;
-            g.shape = b->shape[model][dir];
-            g.offset = (int)all.size();
-            const Shape sh = dir == DIR_X ? kShapesX[g.shape] : shape_y[model];
-            g.rows = sh.ts;
-            for (int idx : order) {
-                const Member& m = b->members[idx];
-                if (m.cfg.model != model || m.final) continue;  // finished: no tiles
-                const int len = dir == DIR_X ? m.cfg.nx : m.cfg.ny;
-                const int wid = dir == DIR_X ? m.cfg.ny : m.cfg.nx;
-                const int along = (len + sh.ts - 1) / sh.ts;
-                const int nt = dir == DIR_X ? insts[idx].tiles_x : insts[idx].tiles_y;
-                for (int t = 0; t < nt; ++t) {
-                    TileEnt e;
-                    e.inst = idx;
-                    e.local = t;
-                    e.a_org = (t % along) * sh.ts - 2;
-                    e.b_org = (t / along) * sh.na;
-                    e.len = len;
-                    e.wid = wid;
-                    e.max_steps = insts[idx].max_steps;
-                    e.active = insts[idx].active;
-                    all.push_back(e);
+        for (int f64 = 0; f64 < 2; ++f64)
+            for (int dir = 0; dir < 2; ++dir) {
+                cfd_batch::Group g;
+                g.model = model;
+                g.fp64 = f64;
+                g.dir = dir;
+                g.shape = f64 ? (dir == DIR_X ? 0 : kMarchShape) : b->shape[model][dir];
+                g.offset = (int)all.size();
+                const Shape sh = dir == DIR_X ? kShapesX[f64 ? 0 : g.shape] : shape_y[model][f64];
+                g.rows = sh.ts;
+                for (int idx : order) {
+                    const Member& m = b->members[idx];
+                    // finished members have no tiles
+                    if (m.cfg.model != model || m.inst.fp64 != f64 || m.final) continue;
+                    const int len = dir == DIR_X ? m.cfg.nx : m.cfg.ny;
+                    const int wid = dir == DIR_X ? m.cfg.ny : m.cfg.nx;
+                    const int along = (len + sh.ts - 1) / sh.ts;
+                    const int nt = dir == DIR_X ? insts[idx].tiles_x : insts[idx].tiles_y;
+                    for (int t = 0; t < nt; ++t) {
+                        TileEnt e;
+                        e.inst = idx;
+                        e.local = t;
+                        e.a_org = (t % along) * sh.ts - 2;
+                        e.b_org = (t / along) * sh.na;
+                        e.len = len;
+                        e.wid = wid;
+                        e.max_steps = insts[idx].max_steps;
+                        e.active = insts[idx].active;
+                        all.push_back(e);
+                    }
                 }
+                g.ntiles = (int)all.size() - g.offset;
+                if (g.ntiles) b->groups.push_back(g);
             }
-            g.ntiles = (int)all.size() - g.offset;
-            if (g.ntiles) b->groups.push_back(g);
-        }
     if ((int)insts.size() > b->d_insts_cap) {
         pool_free(b->d_insts, b->stream);
         b->d_insts = nullptr;
@@ -527,7 +617,12 @@ int enqueue_tick(cfd_batch* b, std::vector<Timed>* timing) {
                 cudaEventRecord(e0, b->stream);
             }
             int grid = b->sms;
-            int r = g.model == CFD_MODEL_EULER
+            int r;
+            if (g.fp64)
+                r = g.model == CFD_MODEL_EULER ? launch_fast<MODEL_EULER>(dir, a, grid, b->stream)
+                                               : launch_fast<MODEL_ALLAIRE>(dir, a, grid, b->stream);
+            else
+                r = g.model == CFD_MODEL_EULER
                         ? launch_shape<MODEL_EULER>(dir, g.shape, a, grid, b->stream)
                         : launch_shape<MODEL_ALLAIRE>(dir, g.shape, a, grid, b->stream);
             if (timing) {
@@ -625,8 +720,9 @@ int cfd_batch_member_bytes(const cfd_config* cfg, size_t* bytes) {
     return CFD_OK;
 }
 
-// Saved state of a member (cfd_batch_restore): packed value and
-// compensation planes (nx * ny cells each, no padding) and its time state.
+// Saved state of a member (cfd_batch_restore): its packed planes (nx * ny
+// cells each, no padding; value and compensation, or the FP64 form's
+// doubles) and its time state.
 struct Restore {
     const CkptHeader* h;
     const float4* q4[2];
@@ -721,6 +817,7 @@ static int add_member(cfd_batch* b, const cfd_config* cfg, const double* host_ic
         if (c.bc[k] == CFD_BC_REFLECTIVE) I.flags |= MF_BC << k;
     I.max_steps = max_steps;
     I.active = 1;
+    I.fp64 = c.precision == CFD_PREC_FP64_FAST;
     // upload: the ghosted FP64 grid (or the device-built SoA state) goes
     // through a temporary staging buffer, followed by the FP64 SoA copy the
     // initial wave-speed reduction reads
@@ -907,8 +1004,8 @@ int cfd_batch_autotune(cfd_batch* b, int steps_per_trial, double* best_ms) {
     if (steps_per_trial < 1) steps_per_trial = 1;
     double best_tick = 0.0;
     for (int model = 0; model < 2; ++model) {
-        bool present = false;
-        for (auto& m : b->members) present |= m.cfg.model == model;
+        bool present = false;  // the mixed form's shapes: the fast FP64 form has one each
+        for (auto& m : b->members) present |= m.cfg.model == model && !m.inst.fp64;
         if (!present) continue;
         for (int dir = 0; dir < 2; ++dir) {
             double best = 1e300;
@@ -926,7 +1023,7 @@ int cfd_batch_autotune(cfd_batch* b, int steps_per_trial, double* best_ms) {
                 double ms = 0.0;
                 for (auto& t : ev) {
                     const auto& g = b->groups[t.group];
-                    if (g.model == model && g.dir == dir) {
+                    if (g.model == model && !g.fp64 && g.dir == dir) {
                         float m = 0.f;
                         cudaEventElapsedTime(&m, t.e0, t.e1);
                         ms += m;
@@ -1189,9 +1286,21 @@ int cfd_batch_save(cfd_batch* b, int id, const char* path) {
         }
     }
     BTRY(cudaStreamSynchronize(b->stream));
-    // packed cells -> planes: values of components 0..nv-1, then their compensations
-    std::vector<float> planes(2 * nv * cells);
-    for (int w = 0; w < 2; ++w)
+    // packed cells -> planes: FP64 members nv planes of doubles; mixed
+    // members the values of components 0..nv-1, then their compensations
+    std::vector<double> planes64(I.fp64 ? nv * cells : 0);
+    for (size_t q = 0; I.fp64 && q < cells; ++q) {
+        double v[6];
+        memcpy(v, &q4[0][q], 16);
+        memcpy(v + 2, &q4[1][q], 16);
+        if (nv == 6) {
+            memcpy(v + 4, &q2[0][q], 8);
+            memcpy(v + 5, &q2[1][q], 8);
+        }
+        for (int k = 0; k < nv; ++k) planes64[k * cells + q] = v[k];
+    }
+    std::vector<float> planes(I.fp64 ? 0 : 2 * nv * cells);
+    for (int w = 0; w < 2 && !I.fp64; ++w)
         for (size_t q = 0; q < cells; ++q) {
             float* p = planes.data() + (size_t)w * nv * cells + q;
             p[0] = q4[w][q].x;
@@ -1207,7 +1316,7 @@ int cfd_batch_save(cfd_batch* b, int id, const char* path) {
     ckpt_init(h);
     h.cfg = c;
     h.cfg.stream = nullptr;
-    h.cfg.precision = CFD_PREC_MIXED;
+    h.cfg.precision = I.fp64 ? CFD_PREC_FP64_FAST : CFD_PREC_MIXED;
     h.nv = nv;
     h.g = c.flux_solver == CFD_FLUX_GODUNOV ? 1 : 2;
     h.n = d.n;
@@ -1219,11 +1328,12 @@ int cfd_batch_save(cfd_batch* b, int id, const char* path) {
     h.mass1 = d.mass1;
     h.mass2 = d.mass2;
     h.max_steps = m->max_steps;
-    h.state_bytes = sizeof(float) * planes.size();
+    h.state_bytes = sizeof(float) * planes.size() + sizeof(double) * planes64.size();
     FILE* f = fopen(path, "wb");
     if (!f) return cfd_fail(CFD_ERR_INVALID, "cannot write %s", path);
     bool ok = fwrite(&h, sizeof h, 1, f) == 1 &&
-              fwrite(planes.data(), sizeof(float), planes.size(), f) == planes.size();
+              fwrite(planes.data(), sizeof(float), planes.size(), f) == planes.size() &&
+              fwrite(planes64.data(), sizeof(double), planes64.size(), f) == planes64.size();
     ok = (fclose(f) == 0) && ok;
     return ok ? CFD_OK : cfd_fail(CFD_ERR_INVALID, "short write to %s", path);
 }
@@ -1236,23 +1346,38 @@ int cfd_batch_restore(cfd_batch* b, const char* path, int max_steps, int* id_out
     int r = ckpt_read_header(f, h);
     const int nv = h.nv;
     const size_t cells = r ? 0 : (size_t)h.cfg.nx * h.cfg.ny;
-    if (!r && (h.cfg.precision != CFD_PREC_MIXED || h.cfg.model != (nv == 4 ? 0 : 1) ||
-               h.state_bytes != sizeof(float) * 2 * nv * cells))
+    const bool f64 = h.cfg.precision == CFD_PREC_FP64_FAST;
+    if (!r && ((h.cfg.precision != CFD_PREC_MIXED && !f64) || h.cfg.model != (nv == 4 ? 0 : 1) ||
+               h.state_bytes != (f64 ? sizeof(double) * nv * cells : sizeof(float) * 2 * nv * cells)))
         r = CFD_ERR_INVALID;
     std::vector<float> planes;
+    std::vector<double> planes64;
     if (!r) {
-        planes.resize(2 * nv * cells);
-        if (fread(planes.data(), sizeof(float), planes.size(), f) != planes.size())
-            r = CFD_ERR_INVALID;
+        if (f64) {
+            planes64.resize(nv * cells);
+            if (fread(planes64.data(), sizeof(double), planes64.size(), f) != planes64.size())
+                r = CFD_ERR_INVALID;
+        } else {
+            planes.resize(2 * nv * cells);
+            if (fread(planes.data(), sizeof(float), planes.size(), f) != planes.size())
+                r = CFD_ERR_INVALID;
+        }
     }
     fclose(f);
-    if (r) return cfd_fail(r, "%s is not a mixed-precision checkpoint", path);
+    if (r) return cfd_fail(r, "%s is not a batch member checkpoint", path);
+    // planes -> packed cells (the FP64 form's doubles in the same bytes)
     std::vector<float4> q4[2];
     std::vector<float2> q2[2];
     for (int w = 0; w < 2; ++w) {
         q4[w].resize(cells);
         if (nv == 6) q2[w].resize(cells);
         for (size_t q = 0; q < cells; ++q) {
+            if (f64) {
+                const double v[2] = {planes64[(2 * w) * cells + q], planes64[(2 * w + 1) * cells + q]};
+                memcpy(&q4[w][q], v, 16);
+                if (nv == 6) memcpy(&q2[w][q], &planes64[(4 + w) * cells + q], 8);
+                continue;
+            }
             const float* p = planes.data() + (size_t)w * nv * cells + q;
             q4[w][q] = make_float4(p[0], p[cells], p[2 * cells], p[3 * cells]);
             if (nv == 6) q2[w][q] = make_float2(p[4 * cells], p[5 * cells]);

@@ -1,8 +1,8 @@
 // Binary checkpoint format of a solve (little-endian, as the host writes it):
 //   CkptHeader
-//   state: plain FP64 solves: nv planes of nx*ny doubles (row-major, no
-//          padding); mixed solves: nv planes of nx*ny floats (values), then
-//          nv planes of their compensation words
+//   state: plain and fast FP64 solves: nv planes of nx*ny doubles
+//          (row-major, no padding); mixed solves: nv planes of nx*ny floats
+//          (values), then nv planes of their compensation words
 //   ghost frame (has_frame): cells x nv doubles (cfd_frame.h order)
 // The header keeps the solve's configuration (stream pointer cleared) and its
 // device time-loop state, so a restored solve continues bit for bit as if it

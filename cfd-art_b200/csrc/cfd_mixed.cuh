@@ -58,6 +58,7 @@ struct Inst {
     int tiles_x, tiles_y;   // tiles of each sweep
     int max_steps;          // stop after this many steps (and at t >= T)
     int active;             // 0: skip
+    int fp64;               // 1: the planes hold FP64 values (fast FP64 form, cfd_fast64.cuh)
 };
 
 // One tile of a launch, precomputed on the host when the membership or the

@@ -11,9 +11,7 @@
 
 namespace cfdic {
 
-// CFD_OK, CFD_ERR_INVALID (unknown case, or recipe for the other model), or
-// CFD_ERR_UNSUPPORTED for the Allaire cases whose volume fraction comes
-// from a per-cell formula (shocked_SF6, TSTM, RMI_SF6, tin_air_implosion).
+// CFD_OK, or CFD_ERR_INVALID (unknown case, or recipe for the other model).
 int case_program(const cfd_config* cfg, const char* test_case, uint64_t seed,
                  std::vector<Op>& ops, Eos& q);
 int recipe_program(const cfd_config* cfg, int recipe, uint64_t seed, int nbubbles,

@@ -20,6 +20,17 @@
 //   BLEND_CIRCLE  W = frac v[0] + (1-frac) c2p(U), U = p2c(W), cells with
 //                 frac = 0 untouched (seeded bubble recipes)
 //   QUADRANTS     U = v[k], k from (x > a[0], y > a[1]) (four-quadrant Riemann problem)
+//   MIXED_CELL    Allaire: material 1 in its pre- or post-shock state by the
+//                 cell centre's x, material 2 where N x N sub-samples fall in
+//                 a rectangle or left of the sine interface
+//                 x = 2.9 - 0.2 sin(2 pi (y + 1/4)) (shocked_SF6, TSTM, RMI_SF6:
+//                 A/sourcecode/allaire_diffuse_io.cpp:659-870)
+//   RING_CELL     Allaire: material 1 blended between an inner and an outer
+//                 state by a sampled circle, material 2 outside a perturbed
+//                 ring r(theta) (tin_air_implosion: A/sourcecode/allaire_diffuse_io.cpp:872-983)
+// The last two call sin / cos / atan2: the host gets the C library's values,
+// the device CUDA's, which agree to an ulp or so; a cell can differ only if
+// one of its sample points lies that close to the interface.
 #pragma once
 
 #include <math.h>
@@ -42,6 +53,8 @@ enum OpKind {
     OP_SET_HALFSPACE = 6,
     OP_BLEND_CIRCLE = 7,
     OP_QUADRANTS = 8,
+    OP_MIXED_CELL = 9,
+    OP_RING_CELL = 10,
 };
 
 struct Op {
@@ -113,6 +126,18 @@ IC_HD void allaire_c2p(const Eos& q, const double* U, double* W) {
     W[5] = z;
 }
 
+// Two-material cell of given volume fraction z of material 1 (partial
+// densities, momentum, energy from each material's specific energy).
+IC_HD void mixed_cell(double z, double rho1, double rho2, double u, double v, double e1, double e2,
+                      double* U) {
+    U[0] = z * rho1;
+    U[1] = (1.0 - z) * rho2;
+    U[2] = u * (z * rho1 + (1.0 - z) * rho2);
+    U[3] = v * (z * rho1 + (1.0 - z) * rho2);
+    U[4] = z * rho1 * e1 + (1.0 - z) * rho2 * e2 + 0.5 * (z * rho1 + (1.0 - z) * rho2) * (u * u + v * v);
+    U[5] = z;
+}
+
 IC_HD int nvar(const Eos& q) { return q.model == 0 ? 4 : 6; }
 
 IC_HD void p2c(const Eos& q, const double* W, double* U) {
@@ -137,8 +162,39 @@ IC_HD bool inside_rect(double sx, double sy, const double* a) {
     sy -= a[1];
     return (0.0 <= sx) & (sx <= a[2]) & (0.0 <= sy) & (sy <= a[3]);
 }
-IC_HD double sample_frac(const Geom& G, double ccx, double ccy, int N, bool circle,
-                         const double* a) {
+// Material-2 regions of MIXED_CELL (a[0..3] = x0, x1, y0, y1 of a closed
+// rectangle, or a[0] = pi for the sine interface) and of RING_CELL
+// (a[0] = pi / 2).
+IC_HD bool inside_box(double sx, double sy, const double* a) {
+    return sx >= a[0] && sx <= a[1] && sy >= a[2] && sy <= a[3];
+}
+IC_HD bool left_of_sine(double sx, double sy, const double* a) {
+    double interfacex = 2.9 - 0.2 * sin(2.0 * a[0] * (sy + 0.25));
+    return interfacex > sx;
+}
+IC_HD bool inside_ring(double sx, double sy, const double* a) {
+    double theta = atan2(sy, sx);
+    theta -= a[0];
+    double r = 20.0 + 0.4 * cos(22 * theta) + 0.4 * cos(17 * theta) + 0.3 * cos(29 * theta);
+    return sqrt(sx * sx + sy * sy) <= r;
+}
+IC_HD bool inside_r24(double sx, double sy, const double*) { return sqrt(sx * sx + sy * sy) <= 24.0; }
+
+enum { REGION_CIRCLE, REGION_RECT, REGION_BOX, REGION_SINE, REGION_RING, REGION_R24 };
+
+IC_HD bool inside_region(int region, double sx, double sy, const double* a) {
+    switch (region) {
+        case REGION_CIRCLE: return inside_circle(sx, sy, a);
+        case REGION_RECT: return inside_rect(sx, sy, a);
+        case REGION_BOX: return inside_box(sx, sy, a);
+        case REGION_SINE: return left_of_sine(sx, sy, a);
+        case REGION_RING: return inside_ring(sx, sy, a);
+        default: return inside_r24(sx, sy, a);
+    }
+}
+
+IC_HD double sample_region(const Geom& G, double ccx, double ccy, int N, int region,
+                           const double* a) {
     int numinside = 0;
     double delx = G.dx / N, dely = G.dy / N;
     double blx = ccx - 0.5 * G.dx, bly = ccy - 0.5 * G.dy;
@@ -146,9 +202,14 @@ IC_HD double sample_frac(const Geom& G, double ccx, double ccy, int N, bool circ
         for (int r = 0; r < N; ++r) {
             double sx = blx + (p + 0.5) * delx;
             double sy = bly + (r + 0.5) * dely;
-            if (circle ? inside_circle(sx, sy, a) : inside_rect(sx, sy, a)) numinside++;
+            if (inside_region(region, sx, sy, a)) numinside++;
         }
     return double(numinside) / (N * N);
+}
+
+IC_HD double sample_frac(const Geom& G, double ccx, double ccy, int N, bool circle,
+                         const double* a) {
+    return sample_region(G, ccx, ccy, N, circle ? REGION_CIRCLE : REGION_RECT, a);
 }
 
 // State of the cell whose centre is at column offset jj and row offset ii
@@ -214,6 +275,29 @@ IC_HD void eval_cell_n(const Op* ops, int nops, const Eos& q, const Geom& G, int
                 bool right = ccx > op.a[0], top = ccy > op.a[1];
                 int s = top ? (right ? 0 : 1) : (right ? 3 : 2);
                 for (int k = 0; k < nv; ++k) U[k] = op.v[s][k];
+                break;
+            }
+            case OP_MIXED_CELL: {
+                // v[0] = pre rho1, u, e1, post rho1, u, e1; v[1] = rho2, e2,
+                // x threshold, +1 (pre where x > it) or -1 (pre where x < it),
+                // region (REGION_BOX or REGION_SINE)
+                const double* m = op.v[0];
+                bool pre = op.v[1][3] > 0.0 ? ccx > op.v[1][2] : ccx < op.v[1][2];
+                double rho1 = pre ? m[0] : m[3], u = pre ? m[1] : m[4], e1 = pre ? m[2] : m[5];
+                double frac = sample_region(G, ccx, ccy, op.n, (int)op.v[1][4], op.a);
+                if constexpr (NV == 6)
+                    mixed_cell(1.0 - frac, rho1, op.v[1][0], u, 0.0, e1, op.v[1][1], U);
+                break;
+            }
+            case OP_RING_CELL: {
+                // v[0] = inner rho1, e1, outer rho1, e1; v[1] = rho2, e2
+                const double* m = op.v[0];
+                double ins = sample_region(G, ccx, ccy, op.n, REGION_R24, op.a);
+                double rho1 = ins * m[0] + (1.0 - ins) * m[2];
+                double e1 = ins * m[1] + (1.0 - ins) * m[3];
+                double frac = sample_region(G, ccx, ccy, op.n, REGION_RING, op.a);
+                if constexpr (NV == 6)
+                    mixed_cell(1.0 - frac, rho1, op.v[1][0], 0.0, 0.0, e1, op.v[1][1], U);
                 break;
             }
             default:

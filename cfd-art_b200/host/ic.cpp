@@ -12,7 +12,8 @@
 // expressed as a shape program (csrc/ic_program.h) that the host evaluates
 // here and the device evaluates in csrc/cfd_ic.cu; the four Allaire cases
 // with their own per-cell formulas (shocked_SF6, TSTM, RMI_SF6,
-// tin_air_implosion) stay host-only.
+// tin_air_implosion) are shape-program operations too (MIXED_CELL,
+// RING_CELL).
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -137,19 +138,6 @@ struct Prog {
 
 // Fraction of N x N sub-cell sample points of cell (i, j) satisfying inside()
 // (E/sourcecode/euler_io.cpp:300-318), for the per-cell Allaire cases.
-template <class F> double sample_frac(const Grid& G, int i, int j, int N, F inside) {
-    int numinside = 0;
-    double delx = G.dx / N, dely = G.dy / N;
-    double blx = G.ccx(j) - 0.5 * G.dx, bly = G.ccy(i) - 0.5 * G.dy;
-    for (int a = 0; a < N; ++a)
-        for (int b = 0; b < N; ++b) {
-            double sx = blx + (a + 0.5) * delx;
-            double sy = bly + (b + 0.5) * dely;
-            if (inside(sx, sy)) numinside++;
-        }
-    return double(numinside) / (N * N);
-}
-
 // E/headers/stiffened_gas_eos.hpp:73-76
 double sg_specific_ie(double g, double pinf, double p, double rho) {
     return (p + g * pinf) / ((g - 1.0) * rho);
@@ -352,16 +340,6 @@ const ACase* allaire_lookup(const std::string& tc) {
 
 // Mixed cell from a volume fraction and two pure-material states
 // (A/sourcecode/allaire_diffuse_io.cpp:691-696).
-void mixed_cell(double z, double rho1, double rho2, double u, double v, double e1, double e2,
-                double* U) {
-    U[0] = z * rho1;
-    U[1] = (1.0 - z) * rho2;
-    U[2] = u * (z * rho1 + (1.0 - z) * rho2);
-    U[3] = v * (z * rho1 + (1.0 - z) * rho2);
-    U[4] = z * rho1 * e1 + (1.0 - z) * rho2 * e2 + 0.5 * (z * rho1 + (1.0 - z) * rho2) * (u * u + v * v);
-    U[5] = z;
-}
-
 bool allaire_per_cell_case(const std::string& tc) {
     return tc == "shocked_SF6" || tc == "TSTM" || tc == "RMI_SF6" || tc == "tin_air_implosion";
 }
@@ -444,79 +422,61 @@ bool allaire_case_program(const std::string& tc, Prog& P) {
 }
 
 // A/sourcecode/allaire_diffuse_io.cpp:640-983: the cases whose volume
-// fraction comes from a per-cell formula (host only).
-void allaire_per_cell_ic(const std::string& tc, const cfdic::Eos& q, Grid& G) {
+// fraction comes from a per-cell formula, as MIXED_CELL / RING_CELL
+// operations of the shape program (csrc/ic_program.h).
+bool allaire_per_cell_program(const std::string& tc, Prog& P) {
+    const cfdic::Eos& q = P.q;
     if (tc == "shocked_SF6" || tc == "TSTM" || tc == "RMI_SF6") {
-        double rpre, ppre, upre, rpost, ppost, upost, rho2, p2;
+        double rpre, ppre, upre, rpost, ppost, upost, rho2, p2, thr, dir;
+        Op& o = P.push(cfdic::OP_MIXED_CELL, 10);
         if (tc == "shocked_SF6") {
             rpre = 1.153; ppre = 9.6856; upre = 0.0;
             rpost = 1.6672; ppost = 16.3256; upost = 1.33273;
             rho2 = 5.805; p2 = 9.6856;
+            thr = 0.05; dir = 1.0;  // pre-shock where x > 0.05
+            o.v[1][4] = cfdic::REGION_BOX;
+            o.a[0] = 0.1, o.a[1] = 0.25, o.a[2] = 0.0, o.a[3] = 0.1;
         } else if (tc == "TSTM") {
             rpre = 0.125; ppre = 0.1; upre = 0.0;
             rpost = 1.0; ppost = 1.0; upost = 0.0;
             rho2 = 1.0; p2 = 0.1;
+            thr = 1.0; dir = 1.0;
+            o.v[1][4] = cfdic::REGION_BOX;
+            o.a[0] = 1.0, o.a[1] = 8.0, o.a[2] = -1.0, o.a[3] = 1.5;
         } else {
             rpre = 1.0; ppre = 1.0; upre = 0.0;
             rpost = 1.411; ppost = 1.628; upost = -0.39;
             rho2 = 5.04; p2 = 1.0;
+            thr = 3.2; dir = -1.0;  // pre-shock where x < 3.2
+            o.v[1][4] = cfdic::REGION_SINE;
+            o.a[0] = std::atan(1.0) * 4.0;
         }
-        double epre = sg_specific_ie(q.g1, q.p1, ppre, rpre);
-        double epost = sg_specific_ie(q.g1, q.p1, ppost, rpost);
-        double e2 = sg_specific_ie(q.g2, q.p2, p2, rho2);
-        double v = 0.0;
-        for (int i = 0; i < G.rows(); ++i)
-            for (int j = 0; j < G.cols(); ++j) {
-                double cx = G.ccx(j);
-                double rho1, u, e1;
-                bool pre;
-                if (tc == "shocked_SF6") pre = cx > 0.05;
-                else if (tc == "TSTM") pre = cx > 1.0;
-                else pre = cx < 3.2;
-                if (pre) { rho1 = rpre; u = upre; e1 = epre; }
-                else { rho1 = rpost; u = upost; e1 = epost; }
-                double frac;
-                if (tc == "shocked_SF6")
-                    frac = sample_frac(G, i, j, 10, [](double sx, double sy) {
-                        return sx >= 0.1 && sx <= 0.25 && sy >= 0.0 && sy <= 0.1;
-                    });
-                else if (tc == "TSTM")
-                    frac = sample_frac(G, i, j, 10, [](double sx, double sy) {
-                        return sx >= 1.0 && sx <= 8.0 && sy >= -1.0 && sy <= 1.5;
-                    });
-                else {
-                    double pi = std::atan(1.0) * 4.0;
-                    frac = sample_frac(G, i, j, 10, [&](double sx, double sy) {
-                        double interfacex = 2.9 - 0.2 * std::sin(2.0 * pi * (sy + 0.25));
-                        return interfacex > sx;
-                    });
-                }
-                double z = 1.0 - frac;
-                mixed_cell(z, rho1, rho2, u, v, e1, e2, G.cell(i, j));
-            }
-    } else if (tc == "tin_air_implosion") {
-        double rpre = 7.28, ppre = 1.0, rpost = 11.84, ppost = 1000000.0;
-        double epre = sg_specific_ie(q.g1, q.p1, ppre, rpre);
-        double epost = sg_specific_ie(q.g1, q.p1, ppost, rpost);
-        double rho2 = 0.001, p2 = 1.0;
-        double e2 = sg_specific_ie(q.g2, q.p2, p2, rho2);
-        for (int i = 0; i < G.rows(); ++i)
-            for (int j = 0; j < G.cols(); ++j) {
-                double ins = sample_frac(G, i, j, 10, [](double sx, double sy) {
-                    return std::sqrt(sx * sx + sy * sy) <= 24.0;
-                });
-                double rho1 = ins * rpre + (1.0 - ins) * rpost;
-                double e1 = ins * epre + (1.0 - ins) * epost;
-                double frac = sample_frac(G, i, j, 10, [](double sx, double sy) {
-                    double theta = std::atan2(sy, sx);
-                    theta -= std::atan(1) * 2;
-                    double r = 20.0 + 0.4 * std::cos(22 * theta) + 0.4 * std::cos(17 * theta) +
-                               0.3 * std::cos(29 * theta);
-                    return std::sqrt(sx * sx + sy * sy) <= r;
-                });
-                mixed_cell(1.0 - frac, rho1, rho2, 0.0, 0.0, e1, e2, G.cell(i, j));
-            }
+        o.v[0][0] = rpre;
+        o.v[0][1] = upre;
+        o.v[0][2] = sg_specific_ie(q.g1, q.p1, ppre, rpre);
+        o.v[0][3] = rpost;
+        o.v[0][4] = upost;
+        o.v[0][5] = sg_specific_ie(q.g1, q.p1, ppost, rpost);
+        o.v[1][0] = rho2;
+        o.v[1][1] = sg_specific_ie(q.g2, q.p2, p2, rho2);
+        o.v[1][2] = thr;
+        o.v[1][3] = dir;
+        return true;
     }
+    if (tc == "tin_air_implosion") {
+        double rpre = 7.28, ppre = 1.0, rpost = 11.84, ppost = 1000000.0;
+        double rho2 = 0.001, p2 = 1.0;
+        Op& o = P.push(cfdic::OP_RING_CELL, 10);
+        o.v[0][0] = rpre;
+        o.v[0][1] = sg_specific_ie(q.g1, q.p1, ppre, rpre);
+        o.v[0][2] = rpost;
+        o.v[0][3] = sg_specific_ie(q.g1, q.p1, ppost, rpost);
+        o.v[1][0] = rho2;
+        o.v[1][1] = sg_specific_ie(q.g2, q.p2, p2, rho2);
+        o.a[0] = std::atan(1) * 2;
+        return true;
+    }
+    return false;
 }
 
 // ------------------------------------------------------------- recipes ---
@@ -609,7 +569,7 @@ int case_program(const cfd_config* cfg, const char* test_case, uint64_t seed,
     Prog P{q, ops};
     if (cfg->model == CFD_MODEL_EULER) return euler_case_program(tc, P, seed) ? CFD_OK : CFD_ERR_INVALID;
     if (!allaire_lookup(tc)) return CFD_ERR_INVALID;
-    if (allaire_per_cell_case(tc)) return CFD_ERR_UNSUPPORTED;
+    if (allaire_per_cell_case(tc)) return allaire_per_cell_program(tc, P) ? CFD_OK : CFD_ERR_INVALID;
     return allaire_case_program(tc, P) ? CFD_OK : CFD_ERR_INVALID;
 }
 
@@ -669,10 +629,6 @@ int cfd_case_ic(const cfd_config* cfg, const char* test_case, uint64_t seed, dou
     std::vector<Op> ops;
     cfdic::Eos q;
     int r = cfdic::case_program(cfg, test_case, seed, ops, q);
-    if (r == CFD_ERR_UNSUPPORTED) {
-        allaire_per_cell_ic(test_case, q, G);
-        return CFD_OK;
-    }
     if (r) return cfd_fail(r, "unknown test case '%s' for model %d", test_case, cfg->model);
     run_program(G, ops, q);
     return CFD_OK;

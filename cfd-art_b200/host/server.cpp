@@ -9,9 +9,9 @@
 // times.  Requests that arrive while others run join the next round, so
 // their work overlaps on the device with the work already there.
 //
-// Mixed precision serves through cfd_batch (one persistent launch per sweep
-// for all members); plain FP64 serves each member with its own cfd_solver on
-// the worker's stream.  No counterpart in the reference (one problem per
+// The mixed and fast FP64 forms serve through cfd_batch (one persistent
+// launch per sweep for all members); the bit-identical FP64 form serves each
+// member with its own cfd_solver on its own stream.  No counterpart in the reference (one problem per
 // process, euler_equations/euler_simulation_code/sourcecode/main.cpp:17-49).
 #include <algorithm>
 #include <chrono>
@@ -120,7 +120,7 @@ struct Request {
     int state = CFD_REQ_QUEUED;
     int error = 0;
     Clock::time_point t_submit, t_admit, t_done;
-    int member = -1;          // batch member id (mixed)
+    int member = -1;          // batch member id (mixed and fast FP64 forms)
     cfd_solver* solver = nullptr;  // FP64
     cudaStream_t stream = nullptr; // FP64: the solve's own stream
     cudaEvent_t ev = nullptr;      // FP64: end of its part of a round
@@ -159,6 +159,11 @@ struct cfd_server {
 
 namespace {
 
+// The mixed and fast FP64 forms run as members of one batch.
+bool batched(const cfd_server* s) {
+    return s->opt.precision == CFD_PREC_MIXED || s->opt.precision == CFD_PREC_FP64_FAST;
+}
+
 size_t fp64_bytes(const cfd_config& c) {
     size_t b = 0;
     cfd_device_bytes(&c, &b);
@@ -172,7 +177,7 @@ void admit(cfd_server* s, std::vector<Request*>& to_start) {
     for (auto it = s->queue.begin(); it != s->queue.end();) {
         Request* r = s->reqs[*it].get();
         size_t need = 0;
-        if (s->opt.precision == CFD_PREC_MIXED) cfd_batch_member_bytes(&r->cfg, &need);
+        if (batched(s)) cfd_batch_member_bytes(&r->cfg, &need);
         else need = fp64_bytes(r->cfg);
         if (need <= free_b) {
             free_b -= need;
@@ -208,7 +213,7 @@ int collect(cfd_server* s, Request* r) {
         r->place(&s->arena, elems);
     }
     int rc;
-    if (s->opt.precision == CFD_PREC_MIXED) {
+    if (batched(s)) {
         rc = cfd_batch_download(s->batch, r->member, r->grid, CFD_LAYOUT_GHOSTED_AOS);
         cfd_batch_remove(s->batch, r->member);
     } else {
@@ -234,9 +239,9 @@ int collect(cfd_server* s, Request* r) {
 void worker_main(cfd_server* s) {
     cudaSetDevice(s->device);
     const int K = std::max(1, s->opt.ticks_per_round);
-    const bool mixed = s->opt.precision == CFD_PREC_MIXED;
+    const bool use_batch = batched(s);  // the mixed or fast FP64 form
     std::vector<Request*> finished;  // found done, grids not yet collected
-    bool gather_pending = false;     // mixed: status read queued after the last round
+    bool gather_pending = false;     // batch: status read queued after the last round
     std::vector<Request*> gathered;  // the solves that read covers
     int slot = 0;                    // event pair of the round being launched
     bool timed[2] = {false, false};
@@ -276,7 +281,7 @@ void worker_main(cfd_server* s) {
         // one round of steps (asynchronous)
         if (!run.empty()) {
             cudaEventRecord(s->ev0[slot], s->stream);
-            if (mixed) {
+            if (use_batch) {
                 if (cfd_batch_step(s->batch, K)) s->worker_error = CFD_ERR_CUDA;
             } else {
                 for (Request* r : run) {
@@ -294,7 +299,7 @@ void worker_main(cfd_server* s) {
         // while the round runs; they join the next round
         for (Request* r : start) {
             int rc;
-            if (mixed) {
+            if (use_batch) {
                 rc = r->recipe ? cfd_batch_add_recipe(s->batch, &r->cfg, r->recipe, r->seed,
                                                       r->nbubbles, r->steps, &r->member)
                                : cfd_batch_add(s->batch, &r->cfg, r->grid, r->steps,
@@ -332,9 +337,9 @@ void worker_main(cfd_server* s) {
                 s->admitted++;
             }
         }
-        // mixed: the status read queued after the previous round (it waits
+        // batch: the status read queued after the previous round (it waits
         // for that round only; this round keeps the GPU busy meanwhile)
-        if (mixed && gather_pending) {
+        if (use_batch && gather_pending) {
             int n = 0;
             const int cap = (int)gathered.size() + 64;
             std::vector<int> ids(cap), steps(cap), fin(cap);
@@ -376,7 +381,7 @@ void worker_main(cfd_server* s) {
             account(slot);
             continue;
         }
-        if (mixed) {
+        if (use_batch) {
             // the status after this round, collected during the next one
             gathered.clear();
             for (Request* r : run)
@@ -424,8 +429,12 @@ int enqueue(cfd_server* s, std::unique_ptr<Request> r, int64_t* id_out) {
     r->t_submit = Clock::now();
     const cfd_config* cfg = &r->cfg;
     size_t need = 0;
-    if (s->opt.precision == CFD_PREC_MIXED) cfd_batch_member_bytes(cfg, &need);
-    else need = fp64_bytes(*cfg);
+    if (batched(s)) {
+        r->cfg.precision = s->opt.precision;  // the member's form
+        cfd_batch_member_bytes(cfg, &need);
+    } else {
+        need = fp64_bytes(*cfg);
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     if (need > s->budget) {
         if (r->arena) {  // give the grid back while holding the lock
@@ -448,7 +457,8 @@ extern "C" {
 
 int cfd_server_create(const cfd_server_options* opt, cfd_server** out) {
     if (!opt || !out) return cfd_fail(CFD_ERR_INVALID, "null argument");
-    if (opt->precision != CFD_PREC_MIXED && opt->precision != CFD_PREC_FP64)
+    if (opt->precision != CFD_PREC_MIXED && opt->precision != CFD_PREC_FP64 &&
+        opt->precision != CFD_PREC_FP64_FAST)
         return cfd_fail(CFD_ERR_INVALID, "bad precision");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -464,7 +474,7 @@ int cfd_server_create(const cfd_server_options* opt, cfd_server** out) {
     s->budget = opt->budget_bytes ? opt->budget_bytes
                                   : (size_t)((opt->budget_fraction > 0 ? opt->budget_fraction : 0.8) *
                                              (double)fr);
-    if (opt->precision == CFD_PREC_MIXED) {
+    if (batched(s)) {
         int rc = cfd_batch_create(s->stream, (size_t)-1 / 2, &s->batch);
         if (rc) {
             delete s;

@@ -36,7 +36,14 @@ extern "C" {
 #define CFD_ERR_BUDGET (-6)      /* request exceeds the device-memory budget */
 
 enum { CFD_MODEL_EULER = 0, CFD_MODEL_ALLAIRE = 1 };
-enum { CFD_PREC_FP64 = 0, CFD_PREC_MIXED = 1 };
+/* CFD_PREC_FP64: plain FP64, bit-identical to the reference.
+ * CFD_PREC_MIXED: FP32 arithmetic with an FP32 compensation word per stored
+ *   component (batch members and the server).
+ * CFD_PREC_FP64_FAST: FP64 arithmetic with contracted multiply-adds and
+ *   refined hardware reciprocals / square roots; matches the reference to a
+ *   relative L1 density error far below 1e-12, not bit for bit (batch members
+ *   and the server). */
+enum { CFD_PREC_FP64 = 0, CFD_PREC_MIXED = 1, CFD_PREC_FP64_FAST = 2 };
 enum { CFD_BC_TRANSMISSIVE = 0, CFD_BC_REFLECTIVE = 1 };
 enum { CFD_LIM_MINMOD = 0, CFD_LIM_VANLEER = 1, CFD_LIM_MC = 2, CFD_LIM_UNLIMITED = 3 };
 enum { CFD_FLUX_MUSCL = 0, CFD_FLUX_GODUNOV = 1 };
@@ -130,10 +137,11 @@ int cfd_upload_device(cfd_solver* s, const double* dev_soa, int n, double t);
  * reference test case (set_ICs, sourcecode/euler_io.cpp:436-731 and
  * A/sourcecode/allaire_diffuse_io.cpp:402-640).  The result is bit-identical
  * to cfd_recipe_ic / cfd_case_ic followed by cfd_upload, without a host grid
- * or a host-to-device copy of the state.  The four Allaire cases with
- * per-cell formulas (shocked_SF6, TSTM, RMI_SF6, tin_air_implosion) return
- * CFD_ERR_UNSUPPORTED: build them with cfd_case_ic.  No counterpart in the
- * reference, which builds every grid on the host. */
+ * or a host-to-device copy of the state.  For the four Allaire cases with
+ * per-cell formulas (shocked_SF6, TSTM, RMI_SF6, tin_air_implosion), which
+ * call sin / cos / atan2, the device's values of those functions decide the
+ * rare sample point that lies within an ulp of an interface.  No
+ * counterpart in the reference, which builds every grid on the host. */
 int cfd_upload_recipe(cfd_solver* s, int recipe, uint64_t seed, int nbubbles, int n, double t);
 int cfd_upload_case(cfd_solver* s, const char* test_case, uint64_t seed, int n, double t);
 
@@ -247,14 +255,18 @@ int cfd_compute_dt_noalloc(const cfd_config* cfg, const double* dev_state, int64
                            int pitch, int n, double t, double* dev_out, void* stream);
 int cfd_noalloc_max_rows(void);
 
-/* ---- batched solves (mixed precision) -------------------------------------
+/* ---- batched solves (mixed and fast FP64 forms) ----------------------------
  * Many independent solves of uneven sizes advanced together: each tick runs
- * one persistent x-sweep launch and one y-sweep launch per model over the
- * tiles of every active member, every member choosing its own dt and
- * stopping on its own (at t >= T or after max_steps).  Members use the mixed
- * form: FP32 reconstruction and Riemann solves, state stored as FP32 plus an
- * FP32 compensation word, FP64 for stiffened-gas pressure recovery, the CFL
- * reduction and time.  No counterpart in the reference, which runs one
+ * one persistent x-sweep launch and one y-sweep launch per model and form
+ * over the tiles of every active member, every member choosing its own dt
+ * and stopping on its own (at t >= T or after max_steps).  A member's form is
+ * its cfg.precision: CFD_PREC_FP64_FAST gives the fast FP64 form (FP64
+ * arithmetic with contracted multiply-adds and refined hardware reciprocals
+ * and square roots, relative L1 density error far below 1e-12 against the
+ * reference), any other value the mixed form: FP32 reconstruction and
+ * Riemann solves, state stored as FP32 plus an FP32 compensation word, FP64
+ * for stiffened-gas pressure recovery, the CFL reduction and time.  Both
+ * take 8 bytes per stored component.  No counterpart in the reference, which runs one
  * problem per process (euler_equations/euler_simulation_code/sourcecode/main.cpp:17-49).
  * Members are admitted against a device-memory budget (bytes; 0 = 80 % of the
  * free memory at creation); cfd_batch_add returns CFD_ERR_BUDGET when a
@@ -319,7 +331,7 @@ int cfd_batch_download(cfd_batch* b, int id, double* host, int layout);
 enum { CFD_REQ_QUEUED = 0, CFD_REQ_RUNNING = 1, CFD_REQ_DONE = 2, CFD_REQ_FAILED = 3 };
 
 typedef struct cfd_server_options {
-    int precision;          /* CFD_PREC_MIXED or CFD_PREC_FP64 */
+    int precision;          /* CFD_PREC_MIXED, CFD_PREC_FP64_FAST (batched) or CFD_PREC_FP64 */
     size_t budget_bytes;    /* device memory for resident solves; 0: budget_fraction */
     double budget_fraction; /* of the free device memory at creation (0: 0.8) */
     int ticks_per_round;    /* steps between admission points (0: 16) */

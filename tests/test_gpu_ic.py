@@ -70,11 +70,16 @@ def test_device_case_godunov_grid():
 
 
 @pytest.mark.parametrize("case", PER_CELL_CASES)
-def test_per_cell_cases_are_host_only(case):
-    cfg = G.case_config(G.ALLAIRE, case, 32, 32)
+def test_device_per_cell_cases_equal_host(case):
+    """The Allaire cases with per-cell formulas (A/sourcecode/allaire_diffuse_io.cpp:659-983)
+    built on the device: equal to the host build (which equals the
+    reference's set_ICs bit for bit), with sin / cos / atan2 from CUDA."""
+    cfg = G.case_config(G.ALLAIRE, case, 96, 80)
+    host = G.case_ic(cfg, case)
     with G.Solver(cfg) as s:
-        with pytest.raises(G.CfdError, match="host only"):
-            s.upload_case(case)
+        s.upload_case(case)
+        dev = s.download(G.SOA)
+    assert _same_bits(dev, _interior_soa(host, 2))
 
 
 def test_recipe_for_wrong_model_rejected():
