@@ -136,7 +136,7 @@ int march64_per_sm() {
     static int per_sm = 0;
     if (!per_sm) {
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, fast::fast_march_kernel<MODEL>, 128, 0);
+            &per_sm, fast::fast_march_kernel<MODEL>, 128, fast::march64_smem_bytes<MODEL>());
         if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     }
     return per_sm;
@@ -155,7 +155,7 @@ int launch_fast(int dir, const MixedArgs& a, int sms, cudaStream_t st) {
     if (dir == DIR_X)
         fast::fast_segment_x_kernel<MODEL><<<(warps + 3) / 4, 128, 0, st>>>(a);
     else
-        fast::fast_march_kernel<MODEL><<<(warps + 3) / 4, 128, 0, st>>>(a);
+        fast::fast_march_kernel<MODEL><<<(warps + 3) / 4, 128, fast::march64_smem_bytes<MODEL>(), st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "fast FP64 sweep launch: %s", cudaGetErrorString(e));
     return CFD_OK;

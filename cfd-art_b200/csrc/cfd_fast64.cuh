@@ -410,28 +410,49 @@ __device__ __forceinline__ void repair(double* N, const double* Uold) {
     }
 }
 
-// FP64 cell of buffer `buf` at element offset `off` (see the storage note).
+// The planes of one state buffer of an FP64 member (see the storage note),
+// held in registers: the stores of a sweep go through pointers the compiler
+// cannot tell apart from the member descriptor, so reading the descriptor's
+// pointers again after every store would cost a global load each time.
+struct Planes64 {
+    double2* a;  // components 0-1
+    double2* b;  // components 2-3
+    double* c;   // Allaire E
+    double* d;   // Allaire z
+};
+
 template <int MODEL>
-__device__ __forceinline__ void load64(const Inst& I, int buf, long long off, double* U) {
-    const double2 a = __ldg(reinterpret_cast<const double2*>(I.q4[buf][0]) + off);
-    const double2 b = __ldg(reinterpret_cast<const double2*>(I.q4[buf][1]) + off);
+__device__ __forceinline__ Planes64 planes64(const Inst& I, int buf) {
+    Planes64 p;
+    p.a = reinterpret_cast<double2*>(I.q4[buf][0]);
+    p.b = reinterpret_cast<double2*>(I.q4[buf][1]);
+    p.c = MODEL == MODEL_ALLAIRE ? reinterpret_cast<double*>(I.q2[buf][0]) : nullptr;
+    p.d = MODEL == MODEL_ALLAIRE ? reinterpret_cast<double*>(I.q2[buf][1]) : nullptr;
+    return p;
+}
+
+// FP64 cell at element offset `off` of a buffer that the sweep only reads.
+template <int MODEL>
+__device__ __forceinline__ void load64(const Planes64& P, long long off, double* U) {
+    const double2 a = __ldg(P.a + off);
+    const double2 b = __ldg(P.b + off);
     U[0] = a.x;
     U[1] = a.y;
     U[2] = b.x;
     U[3] = b.y;
     if constexpr (MODEL == MODEL_ALLAIRE) {
-        U[4] = __ldg(reinterpret_cast<const double*>(I.q2[buf][0]) + off);
-        U[5] = __ldg(reinterpret_cast<const double*>(I.q2[buf][1]) + off);
+        U[4] = __ldg(P.c + off);
+        U[5] = __ldg(P.d + off);
     }
 }
 
 template <int MODEL>
-__device__ __forceinline__ void store64(const Inst& I, int buf, long long off, const double* U) {
-    reinterpret_cast<double2*>(I.q4[buf][0])[off] = make_double2(U[0], U[1]);
-    reinterpret_cast<double2*>(I.q4[buf][1])[off] = make_double2(U[2], U[3]);
+__device__ __forceinline__ void store64(const Planes64& P, long long off, const double* U) {
+    P.a[off] = make_double2(U[0], U[1]);
+    P.b[off] = make_double2(U[2], U[3]);
     if constexpr (MODEL == MODEL_ALLAIRE) {
-        reinterpret_cast<double*>(I.q2[buf][0])[off] = U[4];
-        reinterpret_cast<double*>(I.q2[buf][1])[off] = U[5];
+        P.c[off] = U[4];
+        P.d[off] = U[5];
     }
 }
 
@@ -451,6 +472,55 @@ __device__ __forceinline__ void speeds(const DPar& P, const double* N, double& s
 }
 
 // ---- y sweep by marching strips ---------------------------------------------
+
+// Rows staged ahead through shared memory: a lane copies the cells of rows
+// k+1 .. k+kAhead of its column global -> shared with cp.async while it
+// computes row k, so no registers are held by the loads in flight.  A ring
+// of kAhead + 1 slots, so the slot refilled at row k is the one read at row
+// k - 1; per slot NU 16-byte units per lane (components 0-1, 2-3, and for
+// Allaire E and z), lane-major.
+constexpr int kAhead = 3, kSlots = kAhead + 1;
+template <int MODEL>
+__host__ __device__ constexpr int stage_units() {
+    return MODEL == MODEL_ALLAIRE ? 3 : 2;
+}
+template <int MODEL>
+__host__ __device__ constexpr int march64_smem_bytes() {
+    return 4 * kSlots * stage_units<MODEL>() * 32 * 16;  // 4 warps per CTA
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Starts copying the cell at element offset `off` into slot `s` of this lane.
+template <int MODEL>
+__device__ __forceinline__ void stage_issue(char* stg, int s, const Planes64& P, long long off) {
+    constexpr int NU = stage_units<MODEL>();
+    mixed::cp_async16(stg + ((s * NU + 0) * 32) * 16, P.a + off);
+    mixed::cp_async16(stg + ((s * NU + 1) * 32) * 16, P.b + off);
+    if constexpr (MODEL == MODEL_ALLAIRE) {
+        mixed::cp_async8(stg + ((s * NU + 2) * 32) * 16, P.c + off);
+        mixed::cp_async8(stg + ((s * NU + 2) * 32) * 16 + 8, P.d + off);
+    }
+}
+
+template <int MODEL>
+__device__ __forceinline__ void stage_read(const char* stg, int s, double* U) {
+    constexpr int NU = stage_units<MODEL>();
+    const double2 a = *reinterpret_cast<const double2*>(stg + ((s * NU + 0) * 32) * 16);
+    const double2 b = *reinterpret_cast<const double2*>(stg + ((s * NU + 1) * 32) * 16);
+    U[0] = a.x;
+    U[1] = a.y;
+    U[2] = b.x;
+    U[3] = b.y;
+    if constexpr (MODEL == MODEL_ALLAIRE) {
+        const double2 c = *reinterpret_cast<const double2*>(stg + ((s * NU + 2) * 32) * 16);
+        U[4] = c.x;
+        U[5] = c.y;
+    }
+}
 // A lane walks up its column from row r0 - 2 to r1 + 1 (two halo rows at each
 // end, mirrored at the domain edges as pre_sweep fills them,
 // E/sourcecode/euler_ppsweep.cpp:7-118).  Loading row k completes the slope
@@ -476,7 +546,9 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
     const int c = min(col, nx - 1);
     const int r0 = g.a_org + 2;
     const int r1 = min(r0 + A.rows, ny);
-    const int bin = g.cur ^ 1, bout = g.cur;  // the x sweep's output -> the current buffer
+    // the x sweep's output -> the current buffer
+    const Planes64 pin = planes64<MODEL>(I, g.cur ^ 1), pout = planes64<MODEL>(I, g.cur);
+    const long long pitch = I.pitch;
     const bool wall_lo = (P.flags >> 7) & 1, wall_hi = (P.flags >> 8) & 1;
     const bool god = P.godunov();
     const int lim = P.limiter();
@@ -505,16 +577,28 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
     for (int q = 0; q < NV; ++q) Q1.W[q] = Q2.W[q] = H1[q] = A2[q] = Pp[q] = 0.0;
     Q1.r = Q1.ie = Q1.kn = Q2.r = Q2.ie = Q2.kn = 0.0;
 
-    double nh[NV];
-    bool nneg;
-    load64<MODEL>(I, bin, (long long)src_row(r0 - 2, nneg) * I.pitch + c, nh);
+    // this lane's staging slots; rows r0-2 .. r0-3+kAhead in flight first
+    extern __shared__ __align__(16) char fast_stage[];
+    char* stg = fast_stage + (threadIdx.x >> 5) * (kSlots * stage_units<MODEL>() * 32 * 16) + 16 * lane;
+    bool dummy;
+#pragma unroll
+    for (int j = 0; j < kAhead; ++j) {
+        if (r0 - 2 + j <= r1 + 1) stage_issue<MODEL>(stg, j, pin, src_row(r0 - 2 + j, dummy) * pitch + c);
+        mixed::cp_async_commit();
+    }
+    int slot = 0;
 
     for (int k = r0 - 2; k <= r1 + 1; ++k) {
         double h[NV];
-#pragma unroll
-        for (int q = 0; q < NV; ++q) h[q] = nh[q];
-        const bool neg = nneg;
-        if (k + 1 <= r1 + 1) load64<MODEL>(I, bin, (long long)src_row(k + 1, nneg) * I.pitch + c, nh);
+        bool neg;
+        src_row(k, neg);
+        cp_async_wait<kAhead - 1>();  // row k has arrived
+        stage_read<MODEL>(stg, slot, h);
+        const int refill = slot == 0 ? kSlots - 1 : slot - 1;  // read at row k - 1
+        if (k + kAhead <= r1 + 1)
+            stage_issue<MODEL>(stg, refill, pin, src_row(k + kAhead, dummy) * pitch + c);
+        mixed::cp_async_commit();
+        slot = slot == kSlots - 1 ? 0 : slot + 1;
         // sweep frame: mirror sign, then (u, v) -> (v, -u) (E/sourcecode/euler_colsweep.cpp:22-29)
         {
             const double m = h[MT::IM], n = neg ? -h[MT::IT] : h[MT::IT];
@@ -562,14 +646,14 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
                 if constexpr (MODEL == MODEL_EULER) {
                     if (!euler_physical(N)) {  // the stored old state, for the restore
                         double Uo[NV];
-                        load64<MODEL>(I, bin, (long long)row * I.pitch + c, Uo);
+                        load64<MODEL>(pin, row * pitch + c, Uo);
                         repair<MODEL>(N, Uo);
                     }
                 } else {
                     repair<MODEL>(N, nullptr);
                 }
                 if (live) {
-                    store64<MODEL>(I, bout, (long long)row * I.pitch + c, N);
+                    store64<MODEL>(pout, row * pitch + c, N);
                     double su, sv, m1, m2;
                     speeds<MODEL>(P, N, su, sv, m1, m2);
                     rmu = dmax(rmu, su);
@@ -624,8 +708,10 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
     }
 }
 
+// Euler bounded to 128 registers for 4 CTAs per SM: its y sweep measured
+// faster than at the 3 CTAs of its unbounded register count; Allaire runs 2.
 template <int MODEL>
-__global__ void __launch_bounds__(128) fast_march_kernel(MixedArgs A) {
+__global__ void __launch_bounds__(128, MODEL == MODEL_EULER ? 4 : 2) fast_march_kernel(MixedArgs A) {
     const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int nw = gridDim.x * (blockDim.x >> 5);
     for (int tile = gw; tile < A.ntiles; tile += nw) {
@@ -660,7 +746,8 @@ __device__ __forceinline__ void segment64_tile(const MixedArgs& A, const TileGeo
     const double s_half = 0.5 * (dt / I.dx);
     const double k_upd = dt / I.dx;
     const int nx = g.len, ny = g.wid;
-    const int bin = g.cur, bout = g.cur ^ 1;
+    const Planes64 pin = planes64<MODEL>(I, g.cur), pout = planes64<MODEL>(I, g.cur ^ 1);
+    const long long pitch = I.pitch;
     const bool god = P.godunov();
     const int lim = P.limiter();
     const double z_min = I.z_min;
@@ -680,12 +767,12 @@ __device__ __forceinline__ void segment64_tile(const MixedArgs& A, const TileGeo
     const int row_end = min(g.b_org + mixed::kSegRows, ny);
 
     double nh[NV];
-    load64<MODEL>(I, bin, (long long)g.b_org * I.pitch + src, nh);
+    load64<MODEL>(pin, g.b_org * pitch + src, nh);
     for (int row = g.b_org; row < row_end; ++row) {
         double h[NV];
 #pragma unroll
         for (int q = 0; q < NV; ++q) h[q] = nh[q];
-        if (row + 1 < row_end) load64<MODEL>(I, bin, (long long)(row + 1) * I.pitch + src, nh);
+        if (row + 1 < row_end) load64<MODEL>(pin, (row + 1) * pitch + src, nh);
         if (neg) h[MT::IM] = -h[MT::IM];
         Prim64<MODEL> Q;
         c2p<MODEL>(P, h, Q);
@@ -731,13 +818,15 @@ __device__ __forceinline__ void segment64_tile(const MixedArgs& A, const TileGeo
             N[5] = z_new(god, k_upd, Wl[5], h[5], Wr[5], F[NV], FR[NV], F[NV + 1], FR[NV + 1], z_min);
         if (writer) {  // interior cells: h is the stored old state
             repair<MODEL>(N, h);
-            store64<MODEL>(I, bout, (long long)row * I.pitch + ga, N);
+            store64<MODEL>(pout, row * pitch + ga, N);
         }
     }
 }
 
+// At least 4 CTAs per SM: Allaire bounded from 144 to 128 registers (24 bytes
+// spill) measured 25 % faster than at 3 CTAs; Euler (96 registers) runs 5.
 template <int MODEL>
-__global__ void __launch_bounds__(128) fast_segment_x_kernel(MixedArgs A) {
+__global__ void __launch_bounds__(128, 4) fast_segment_x_kernel(MixedArgs A) {
     const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int nw = gridDim.x * (blockDim.x >> 5);
     for (int tile = gw; tile < A.ntiles; tile += nw) {

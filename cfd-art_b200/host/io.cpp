@@ -73,6 +73,7 @@ int wavespeed_of(const std::string& s) {
 int precision_of(const std::string& s) {
     if (s == "fp64") return CFD_PREC_FP64;
     if (s == "mixed") return CFD_PREC_MIXED;
+    if (s == "fp64_fast") return CFD_PREC_FP64_FAST;
     return -1;
 }
 
@@ -170,7 +171,7 @@ int cfd_settings_config(const cfd_settings* s, cfd_config* cfg) {
                         s->wavespeed);
     int prec = s->precision[0] ? precision_of(s->precision) : CFD_PREC_FP64;
     if (prec < 0)
-        return cfd_fail(CFD_ERR_INVALID, "settings: unknown precision '%s' (fp64, mixed)",
+        return cfd_fail(CFD_ERR_INVALID, "settings: unknown precision '%s' (fp64, mixed, fp64_fast)",
                         s->precision);
     int r;
     int rec = recipe_of(s->test_case);
