@@ -5,7 +5,9 @@
 // along its line one cell at a time, carrying the window the stencil needs
 // from one row to the next (primitive states, face states, raw cells, flux;
 // in registers, or for the six-component Allaire model partly in a per-lane
-// column of shared memory).  The strip length is chosen per launch on the
+// column of shared memory).  The rows ahead of the one being computed are
+// copied global -> shared with cp.async, three rows in flight, so no
+// registers are held by the loads.  The strip length is chosen per launch on the
 // host (kMarchMinRows..kMarchMaxRows) so that the strips fill the resident
 // warps.  No barrier is needed, and only the two halo cells at each end of
 // a strip are re-read.  In the y sweep the lanes are 32 consecutive columns,
@@ -118,10 +120,25 @@ constexpr bool march_win_smem() {
     return MODEL == MODEL_ALLAIRE;
 }
 
-// Dynamic shared memory of a 4-warp marching CTA.
+// Rows staged ahead through shared memory with cp.async (no registers held
+// by the loads in flight): a ring of kMSlots slots, kMAhead rows in flight,
+// per slot MU 16-byte units per lane (value and compensation words of
+// components 0-3; for Allaire E and z with their compensation words).
+constexpr int kMAhead = 3, kMSlots = kMAhead + 1;
 template <int MODEL>
-constexpr int march_smem_bytes() {
+__host__ __device__ constexpr int march_units() {
+    return MODEL == MODEL_ALLAIRE ? 3 : 2;
+}
+
+// Dynamic shared memory of a 4-warp marching CTA: the carried window
+// (Allaire), then the staging ring.
+template <int MODEL>
+__host__ __device__ constexpr int march_win_bytes() {
     return march_win_smem<MODEL>() ? 4 * 8 * ModelTraits<MODEL>::NV * 32 * (int)sizeof(float) : 0;
+}
+template <int MODEL>
+__host__ __device__ constexpr int march_smem_bytes() {
+    return march_win_bytes<MODEL>() + 4 * kMSlots * march_units<MODEL>() * 32 * 16;
 }
 
 template <int MODEL, bool SMEM = march_win_smem<MODEL>()>
@@ -253,21 +270,47 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
 #pragma unroll
     for (int q = 0; q < NV; ++q) W1[q] = W2[q] = 0.f;
 
-    // next row's raw cell, loaded one iteration ahead (in registers: on
-    // this kernel a shared-memory staging of the rows ahead measured slower)
-    float nh[NV], nl[NV];
-    bool nneg;
-    march_load<MODEL, DIR>(I, bin, src_row(r0 - 2, nneg), c, nh, nl);
+    // rows staged ahead (y sweep: line = column, along = row)
+    extern __shared__ __align__(16) char march_stage[];
+    constexpr int MU = march_units<MODEL>();
+    char* stg = march_stage + march_win_bytes<MODEL>() + (threadIdx.x >> 5) * (kMSlots * MU * 32 * 16) +
+                16 * lane;
+    auto issue = [&](int s, int k) {
+        bool ng;
+        const long long off = (long long)src_row(k, ng) * I.pitch + c;
+        cp_async16(stg + ((s * MU + 0) * 32) * 16, I.q4[bin][0] + off);
+        cp_async16(stg + ((s * MU + 1) * 32) * 16, I.q4[bin][1] + off);
+        if constexpr (MODEL == MODEL_ALLAIRE) {
+            cp_async8(stg + ((s * MU + 2) * 32) * 16, I.q2[bin][0] + off);
+            cp_async8(stg + ((s * MU + 2) * 32) * 16 + 8, I.q2[bin][1] + off);
+        }
+    };
+#pragma unroll
+    for (int j = 0; j < kMAhead; ++j) {
+        if (r0 - 2 + j <= r1 + 1) issue(j, r0 - 2 + j);
+        cp_async_commit();
+    }
+    int slot = 0;
 
     for (int k = r0 - 2; k <= r1 + 1; ++k) {
         float h[NV], l[NV];
-#pragma unroll
-        for (int q = 0; q < NV; ++q) {
-            h[q] = nh[q];
-            l[q] = nl[q];
+        bool neg;
+        src_row(k, neg);
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kMAhead - 1) : "memory");
+        {
+            const float4 a = *reinterpret_cast<const float4*>(stg + ((slot * MU + 0) * 32) * 16);
+            const float4 b = *reinterpret_cast<const float4*>(stg + ((slot * MU + 1) * 32) * 16);
+            h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w;
+            l[0] = b.x; l[1] = b.y; l[2] = b.z; l[3] = b.w;
+            if constexpr (MODEL == MODEL_ALLAIRE) {
+                const float4 e = *reinterpret_cast<const float4*>(stg + ((slot * MU + 2) * 32) * 16);
+                h[4] = e.x; h[5] = e.y;
+                l[4] = e.z; l[5] = e.w;
+            }
         }
-        const bool neg = nneg;
-        if (k + 1 <= r1 + 1) march_load<MODEL, DIR>(I, bin, src_row(k + 1, nneg), c, nh, nl);
+        if (k + kMAhead <= r1 + 1) issue(slot == 0 ? kMSlots - 1 : slot - 1, k + kMAhead);
+        cp_async_commit();
+        slot = slot == kMSlots - 1 ? 0 : slot + 1;
         march_frame_in<MODEL, DIR>(h, l, neg);
         win.put_raw(h, l);
         float W0[NV];
