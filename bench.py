@@ -211,6 +211,17 @@ def served_requests(n: int, seed: int):
     return out
 
 
+# The batched instances take the y sweep's MUSCL-Hancock half step on dy.
+# Their cells are up to 16 times longer one way than the other, and the
+# reference's half step on dx in the y sweep (E/sourcecode/euler_colsweep.cpp:43)
+# makes those runs ill-conditioned where dx is several times dy: round-off
+# grows until even two FP64 forms of the same scheme (bit-identical and fast)
+# differ by a few per cent after 500 steps, while with the dy half step
+# every form agrees with the others to about 1e-6.  Every other workload has
+# square cells, where the two half steps are the same.
+BATCH_FIX_DY = 1
+
+
 def batch_instances(n: int, seed: int):
     """Batched config: Euler instances with nx, ny log-uniform in [64, 1024]
     and 4-16 bubbles each, 500 steps."""
@@ -260,17 +271,18 @@ REF_UNIT_CELLS = {"euler": 1.6e7, "allaire": 6e6}
 
 def reference_units(workload: str, count: int):
     """The workload's units as the reference's CPU code runs them:
-    (recipe, nx, ny, seed, nbubbles, steps).  served: the repo arm's request
-    stream (same seeds; warm-up requests first); batch256: its instances;
-    single-grid workloads: the grid itself, `steps` = 1 per unit."""
+    (recipe, nx, ny, seed, nbubbles, steps, fix_dy_halfstep).  served: the
+    repo arm's request stream (same seeds; warm-up requests first);
+    batch256: its instances; single-grid workloads: the grid itself,
+    `steps` = 1 per unit."""
     if workload == "served":
-        return [(rec, nx, ny, sd, nb, steps)
+        return [(rec, nx, ny, sd, nb, steps, 0)
                 for (_, rec, nx, ny, steps, sd, nb) in served_requests(count, SEED)]
     if workload == "batch256":
-        return [(r, nx, ny, sd, nb, steps)
+        return [(r, nx, ny, sd, nb, steps, BATCH_FIX_DY)
                 for r, nx, ny, steps, sd, nb in batch_instances(256, SEED)][:count]
     recipe, nx, ny, nbub, _prec = SINGLE[workload]
-    return [(recipe, nx, ny, SEED, nbub, 1)]
+    return [(recipe, nx, ny, SEED, nbub, 1, 0)]
 
 
 class RefRunner:
@@ -293,8 +305,9 @@ class RefRunner:
             f.restype = ctypes.c_double
             self.secs[model] = f
 
-    def unit(self, recipe, nx, ny, seed, nb, steps, cap=True):
+    def unit(self, recipe, nx, ny, seed, nb, steps, fix_dy=0, cap=True):
         grid, p, model = self.O.port_recipe_ic(recipe, nx, ny, seed, nb)
+        p.fix_dy_halfstep = fix_dy
         if cap:
             steps = max(2, min(steps, int(REF_UNIT_CELLS[model] // (nx * ny))))
         taken, _, _, _ = self.O.ref_run(model, p, grid, steps, threads=self.threads)
@@ -334,12 +347,12 @@ def cpu_baseline(workload: str, budget_s: float = 16.0, single_thread_s: float =
         R = RefRunner(threads)
         cells = secs = 0.0
         units = taken_steps = 0
-        for (rec, nx, ny, sd, nb, steps) in reference_units(workload, 64):
+        for (rec, nx, ny, sd, nb, steps, fix) in reference_units(workload, 64):
             nx, ny = max(16, nx // shrink), max(16, ny // shrink)
             if workload in SINGLE:
-                c, s, k, _ = R.unit(rec, nx, ny, sd, nb, 1 << 30)
+                c, s, k, _ = R.unit(rec, nx, ny, sd, nb, 1 << 30, fix)
             else:
-                c, s, k, _ = R.unit(rec, nx, ny, sd, nb, steps)
+                c, s, k, _ = R.unit(rec, nx, ny, sd, nb, steps, fix)
             cells += c
             secs += s
             units += 1
@@ -381,7 +394,7 @@ def run_reference(args) -> None:
     w, K, W = args.workload, args.steps, args.warmup
     cells = secs = 0.0
     if w in SINGLE:
-        rec, nx, ny, sd, nb, _ = reference_units(w, 1)[0]
+        rec, nx, ny, sd, nb, _, _ = reference_units(w, 1)[0]
         for c, s in R.grid_steps(rec, nx, ny, sd, nb, W, K):
             cells += c
             secs += s
@@ -595,6 +608,8 @@ def bench_batch(args, ctx, G, stream, clocks):
     torch = ctx.torch
     insts = batch_instances(256, SEED + 1000 * ctx.rank)
     ics = [build_ic(G, r, nx, ny, sd, nb) for r, nx, ny, steps, sd, nb in insts]
+    for c, _ in ics:
+        c.fix_dy_halfstep = BATCH_FIX_DY
     cells = sum(c.nx * c.ny for c, _ in ics)
     K, W = args.steps, args.warmup
     b = G.Batch(stream=stream.cuda_stream)
@@ -673,6 +688,7 @@ def bench_batch(args, ctx, G, stream, clocks):
             "accuracy_vs_fp64": acc,
             "config": {"workload": "batch256", "model": "euler", "precision": "mixed",
                        "instances": 256, "cells": cells, "sizes": "nx, ny log-uniform [64, 1024]",
+                       "y_half_step": "dy (fix_dy_halfstep; see BATCH_FIX_DY)",
                        "bubbles": "4-16 per instance", "steps_per_instance": 500,
                        "tile_shapes": list(shapes), "autotune_tick_ms": tune_ms,
                        "autotune_steps": sum(pre.values()), "graph": "8 ticks per CUDA graph",

@@ -230,3 +230,26 @@ def test_budget_admission():
         assert n == 2 and used <= budget
         b.remove(a1)
         assert b.try_add(cfg, ic, 10) is not None
+
+
+def test_batch_forms_on_anisotropic_cells_with_dy_half_step():
+    """Cells 4.6 times longer in x than in y (144 x 662 on the unit square,
+    as in the batched workload) over 500 steps, with the y sweep's half step
+    on dy: the mixed form within its bound and the fast FP64 form within the
+    plain form's, against the bit-identical form.  (With the reference's dx
+    half step, E/sourcecode/euler_colsweep.cpp:43, such a run is
+    ill-conditioned: round-off grows to per cent between any two forms.)"""
+    cfg = G.recipe_config("shock_bubbles", 144, 662)
+    cfg.fix_dy_halfstep = 1
+    ic = G.recipe_ic(cfg, "shock_bubbles", nbubbles=8)
+    ref, sr = _fp64_run(cfg, ic, 500)
+    out, sm = _mixed_run(cfg, ic, 500)
+    fast_cfg = cfg.copy()
+    fast_cfg.precision = G.FP64_FAST
+    fast, sf = _mixed_run(fast_cfg, ic, 500)
+    assert sm.n == sf.n == sr.n == 500
+    l1_m, _ = _errors(out, ref, "euler")
+    l1_f, _ = _errors(fast, ref, "euler")
+    print(f"144x662 dy half step, 500 steps: mixed L1 {l1_m:.2e}, fast FP64 L1 {l1_f:.2e}")
+    assert l1_m <= TOL_MIXED_L1
+    assert l1_f <= 1e-12
