@@ -110,6 +110,24 @@ def test_settings_file_roundtrip(tmp_path):
     assert np.array_equal(grid, G.case_ic(cfg, "totem_pole_3"))
 
 
+def test_settings_precision_fp64_fast(tmp_path):
+    """`precision fp64_fast` selects the fast FP64 form (a batch member's
+    form); a single solver rejects it, before any device call, as it rejects
+    the mixed form."""
+    f = tmp_path / "settingsfile.txt"
+    f.write_text("Nx 64\nNy 64\nCFL 0.8\nsplitting_scheme naive_splitting\n"
+                 "test_case shock_bubbles\noutput_freq 0\noutputpath o/\n"
+                 "flux_solver MUSCL\nriemann_solver HLLC\nproblem euler\nprecision fp64_fast\n")
+    L = G.lib()
+    st = G.Settings()
+    assert L.cfd_read_settings(str(f).encode(), C.byref(st)) == 0
+    cfg = G.Config()
+    assert L.cfd_settings_config(C.byref(st), C.byref(cfg)) == 0
+    assert cfg.precision == G.FP64_FAST
+    with pytest.raises(G.CfdError, match="batch members"):
+        G.Solver(cfg)
+
+
 def test_settings_extensions(tmp_path):
     f = tmp_path / "settingsfile.txt"
     f.write_text("Nx 64\nNy 32\nCFL 0.6\nsplitting_scheme strang_splitting\n"
