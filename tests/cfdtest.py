@@ -9,6 +9,31 @@ import oracle_py as O
 
 ROOT = Path(__file__).resolve().parents[1]
 GOLDEN = ROOT / "tests" / "golden"
+# (model, reference test case, nx, ny, steps, configuration overrides) run
+# against the oracle: every limiter, both splittings, Godunov, PVRS speeds,
+# the alpha clip, the dy half step, walls, tiny and ragged grids
+PARITY_CASES = [
+    ("euler", "totem_pole_3", 30, 61, 80, {}),
+    ("euler", "multiple_circles_1", 67, 35, 40, {"limiter": 1}),
+    ("euler", "cross", 129, 70, 30, {"limiter": 2, "cfl": 0.8}),
+    ("euler", "totem_pole_1", 33, 24, 30, {"limiter": 3}),
+    ("euler", "totem_pole_3", 30, 61, 30, {"fix_dy_halfstep": 1}),
+    ("euler", "circular_explosion", 26, 30, 30, {"splitting": 1}),
+    ("euler", "totem_pole_2", 20, 21, 30, {"flux_solver": 1}),
+    ("euler", "circular_explosion", 2, 2, 10, {}),
+    ("euler", "cross", 2, 50, 20, {}),
+    ("euler", "cross", 50, 3, 20, {}),
+    ("allaire", "ST2_y", 10, 60, 50, {}),
+    ("allaire", "TTC3_x_pure", 60, 8, 40, {"limiter": 2}),
+    ("allaire", "circular_explosion", 30, 30, 20, {"limiter": 1}),
+    ("allaire", "shocked_helium_bubble", 40, 20, 20, {}),
+    ("allaire", "underwater_explosion_modified", 32, 32, 20, {}),
+    ("allaire", "tin_air_implosion", 24, 48, 10, {}),
+    ("allaire", "ST2_x", 60, 10, 40, {"wavespeed": 1, "z_min": 1e-6}),
+    ("allaire", "ST1_x", 40, 6, 20, {"flux_solver": 1}),
+    ("allaire", "RMI_SF6", 64, 16, 20, {"splitting": 1}),
+]
+
 # face known-answer fixtures of the reference build (make_golden.py)
 KATS = ["kat_faces_euler", "kat_faces_allaire", "kat_faces_euler_low_energy",
         "kat_faces_allaire_low_energy"]

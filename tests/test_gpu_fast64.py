@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 import cfdgpu as G
-from cfdtest import GOLDEN, config_from_params, density, ghost_grid, load_golden, params_from, rel_l1
+from cfdtest import (GOLDEN, PARITY_CASES, config_from_params, density, ghost_grid, load_golden,
+                     params_from, rel_l1)
 
 pytestmark = pytest.mark.gpu
 TOL_L1 = 1e-12  # relative L1 density error bound of the plain FP64 form
@@ -61,6 +62,33 @@ def test_fast64_matches_reference_run(name):
     assert abs(st.t - float(fx["t"])) <= 1e-12 * max(1.0, abs(float(fx["t"])))
     l1, linf = _errors(out[g:-g, g:-g], _final_state(fx), model)
     print(f"{name}: fast FP64 vs reference L1 {l1:.2e} Linf {linf:.2e}")
+    assert l1 <= TOL_L1
+
+
+@pytest.mark.parametrize("model,case,nx,ny,steps,over",
+                         [c for c in PARITY_CASES if c[5].get("splitting") != 1])
+def test_fast64_matches_bit_exact_on_reference_cases(model, case, nx, ny, steps, over):
+    """The bit-identical form's parity cases (the batch runs naive
+    splitting): every limiter, Godunov, PVRS speeds, the alpha clip, the dy
+    half step, walls, 2x2 / 2x50 / 50x3 grids."""
+    fs = "Godunov" if over.get("flux_solver") == 1 else "MUSCL"
+    cfg = G.case_config(G.EULER if model == "euler" else G.ALLAIRE, case, nx, ny, fs)
+    cfg.cfl = over.get("cfl", 0.5)
+    for k, v in over.items():
+        if k != "cfl":
+            setattr(cfg, k, v)
+    ic = G.case_ic(cfg, case)
+    g = 1 if fs == "Godunov" else 2
+    with G.Solver(cfg) as s:
+        s.upload(ic)
+        s.advance(steps)
+        ref, sr = s.download(), s.status()
+    out, sf = _fast_run(cfg, ic, steps)
+    assert sf.n == sr.n
+    assert abs(sf.t - sr.t) <= 1e-12 * max(abs(sr.t), 1e-300)
+    l1, linf = _errors(out[g:-g, g:-g], ref[g:-g, g:-g], model)
+    print(f"{model} {case} {nx}x{ny} {over}: fast FP64 vs bit-exact L1 {l1:.2e} Linf {linf:.2e}")
+    assert np.isfinite(out[g:-g, g:-g]).all()
     assert l1 <= TOL_L1
 
 
