@@ -180,6 +180,7 @@ def lib() -> C.CDLL:
             "cfd_batch_get_shapes": (ip, [vp, ip, C.POINTER(ip), C.POINTER(ip)]),
             "cfd_batch_set_march_rows": (ip, [vp, ip, ip]),
             "cfd_batch_get_march_rows": (ip, [vp, ip, C.POINTER(ip)]),
+            "cfd_batch_get_segment_rows": (ip, [vp, ip, ip, C.POINTER(ip)]),
             "cfd_batch_status": (ip, [vp, ip, C.POINTER(Status)]),
             "cfd_batch_poll_issue": (ip, [vp]),
             "cfd_batch_poll_collect": (ip, [vp, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip), dp,
@@ -508,6 +509,13 @@ class Batch:
     def march_rows(self, model: int) -> int:
         r = C.c_int()
         check(lib().cfd_batch_get_march_rows(self._h, model, C.byref(r)), "cfd_batch_get_march_rows")
+        return r.value
+
+    def segment_rows(self, model: int, precision: int = MIXED) -> int:
+        """Rows of the x sweep's warp-segment tiles in the current tile list."""
+        r = C.c_int()
+        check(lib().cfd_batch_get_segment_rows(self._h, model, precision, C.byref(r)),
+              "cfd_batch_get_segment_rows")
         return r.value
 
     def status(self, mid: int) -> Status:

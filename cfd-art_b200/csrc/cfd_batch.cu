@@ -55,9 +55,10 @@ namespace {
 struct Shape {
     int ts, na;
 };
-// x: warp segments of kSegCells columns x kSegRows rows (cfd_march.cuh), the
-// only x form (it measured 13-25 % faster than every tile shape, and a single
-// x form keeps results independent of the autotuner's choice).
+// x: warp segments of kSegCells columns (cfd_march.cuh), the only x form (it
+// measured 13-25 % faster than every tile shape, and a single x form keeps
+// results independent of the autotuner's choice); their row count is chosen
+// per launch (seg_rows), kSegRows is the nominal one.
 // y: three tile shapes, and shape 3 = marching strips of 32 columns
 // (cfd_march.cuh), bit-identical to the tiles; their length is chosen per
 // launch (march_rows), kMarchMaxRows is the nominal one.
@@ -115,14 +116,19 @@ int launch_march(const MixedArgs& a, int sms, cudaStream_t st) {
 
 // Persistent warp-segment x sweep (4-warp CTAs), launched like the marching one.
 template <int MODEL>
-int launch_segment(const MixedArgs& a, int sms, cudaStream_t st) {
+int segment_per_sm() {
     static int per_sm = 0;
     if (!per_sm) {
         cudaError_t e =
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_segment_x_kernel<MODEL>, 128, 0);
         if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     }
-    const int warps = std::max(1, std::min(a.ntiles, per_sm * sms * 4));
+    return per_sm;
+}
+
+template <int MODEL>
+int launch_segment(const MixedArgs& a, int sms, cudaStream_t st) {
+    const int warps = std::max(1, std::min(a.ntiles, segment_per_sm<MODEL>() * sms * 4));
     mixed_segment_x_kernel<MODEL><<<(warps + 3) / 4, 128, 0, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "segment launch: %s", cudaGetErrorString(e));
@@ -143,14 +149,19 @@ int march64_per_sm() {
 }
 
 template <int MODEL>
-int launch_fast(int dir, const MixedArgs& a, int sms, cudaStream_t st) {
-    static int seg_per_sm = 0;
-    if (dir == DIR_X && !seg_per_sm) {
+int segment64_per_sm() {
+    static int per_sm = 0;
+    if (!per_sm) {
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &seg_per_sm, fast::fast_segment_x_kernel<MODEL>, 128, 0);
-        if (e != cudaSuccess || seg_per_sm < 1) seg_per_sm = 1;
+            &per_sm, fast::fast_segment_x_kernel<MODEL>, 128, 0);
+        if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     }
-    const int per_sm = dir == DIR_X ? seg_per_sm : march64_per_sm<MODEL>();
+    return per_sm;
+}
+
+template <int MODEL>
+int launch_fast(int dir, const MixedArgs& a, int sms, cudaStream_t st) {
+    const int per_sm = dir == DIR_X ? segment64_per_sm<MODEL>() : march64_per_sm<MODEL>();
     const int warps = std::max(1, std::min(a.ntiles, per_sm * sms * 4));
     if (dir == DIR_X)
         fast::fast_segment_x_kernel<MODEL><<<(warps + 3) / 4, 128, 0, st>>>(a);
@@ -190,6 +201,29 @@ int march_rows(const std::vector<std::pair<int, int>>& grids, long long slots) {
         for (const auto& g : grids) strips += (long long)((g.first + 31) / 32) * ((g.second + rows - 1) / rows);
         if (!strips) return kMarchMaxRows;
         const long long cost = (strips + slots - 1) / slots * (rows + 4);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = rows;
+        }
+    }
+    return best;
+}
+
+// Row count of the x sweep's warp segments over the given grids: tiles of
+// kSegCells columns, a warp walks ceil(tiles / slots) of them one after the
+// other, each costing its rows plus about two rows' worth of setup (the
+// member's constants, the first row's load), so the count with the fewest
+// (rounds x (rows + 2)) is taken, the largest on ties.  A lone grid that
+// leaves resident warps idle at 32 rows gets shorter tiles.
+int seg_rows(const std::vector<std::pair<int, int>>& grids, long long slots) {
+    int best = kSegRows;
+    long long best_cost = -1;
+    for (int rows = kSegRows; rows >= kSegMinRows; rows -= 2) {
+        long long tiles = 0;
+        for (const auto& g : grids)
+            tiles += (long long)((g.first + kSegCells - 1) / kSegCells) * ((g.second + rows - 1) / rows);
+        if (!tiles) return kSegRows;
+        const long long cost = (tiles + slots - 1) / slots * (rows + 2);
         if (best_cost < 0 || cost < best_cost) {
             best_cost = cost;
             best = rows;
@@ -448,6 +482,7 @@ struct cfd_batch {
     int march_fixed[2] = {0, 0};  // strip length set by the caller (0: chosen per tile list)
     int march_used[2] = {0, 0};   // strip length of the current mixed tile list
     int march_used64[2] = {0, 0}; // strip length of the current fast FP64 tile list
+    int seg_used[2][2] = {};      // [model][fast FP64] rows of the current x segments
     int sms = 148;
     // graph of `graph_steps` ticks for the current membership
     cudaGraphExec_t graph = nullptr;
@@ -488,21 +523,31 @@ int build_tables(cfd_batch* b) {
     if (int r = wait_uploads(b)) return r;
     if (!b->dirty) return CFD_OK;
     b->groups.clear();
-    // the y shape of each (model, form), with the strip length of a marching
-    // sweep; the fast FP64 form always marches in y
-    Shape shape_y[2][2];
+    // the x segments' row count and the y shape of each (model, form), with
+    // the strip length of a marching sweep; the fast FP64 form always
+    // marches in y
+    Shape shape_x[2][2], shape_y[2][2];
     for (int model = 0; model < 2; ++model)
         for (int f64 = 0; f64 < 2; ++f64) {
             const int shp = f64 ? kMarchShape : b->shape[model][DIR_Y];
+            shape_x[model][f64] = kShapesX[0];
             shape_y[model][f64] = kShapesY[shp];
             int& used = f64 ? b->march_used64[model] : b->march_used[model];
             used = 0;
-            if (shp != kMarchShape) continue;
+            b->seg_used[model][f64] = 0;
             std::vector<std::pair<int, int>> grids;
             for (const Member& m : b->members)
                 if (m.cfg.model == model && m.inst.fp64 == f64 && !m.final)
                     grids.emplace_back(m.cfg.nx, m.cfg.ny);
             if (grids.empty()) continue;
+            const int seg_sm =
+                f64 ? (model == CFD_MODEL_EULER ? segment64_per_sm<MODEL_EULER>()
+                                                : segment64_per_sm<MODEL_ALLAIRE>())
+                    : (model == CFD_MODEL_EULER ? segment_per_sm<MODEL_EULER>()
+                                                : segment_per_sm<MODEL_ALLAIRE>());
+            shape_x[model][f64].na = seg_rows(grids, (long long)seg_sm * b->sms * 4);
+            b->seg_used[model][f64] = shape_x[model][f64].na;
+            if (shp != kMarchShape) continue;
             const int per_sm =
                 f64 ? (model == CFD_MODEL_EULER ? march64_per_sm<MODEL_EULER>()
                                                 : march64_per_sm<MODEL_ALLAIRE>())
@@ -517,8 +562,7 @@ int build_tables(cfd_batch* b) {
     for (size_t i = 0; i < b->members.size(); ++i) {
         Member& m = b->members[i];
         int model = m.cfg.model;
-        const int shx = m.inst.fp64 ? 0 : b->shape[model][DIR_X];
-        m.inst.tiles_x = tiles_for(m.cfg.nx, m.cfg.ny, DIR_X, kShapesX[shx]);
+        m.inst.tiles_x = tiles_for(m.cfg.nx, m.cfg.ny, DIR_X, shape_x[model][m.inst.fp64]);
         m.inst.tiles_y = tiles_for(m.cfg.nx, m.cfg.ny, DIR_Y, shape_y[model][m.inst.fp64]);
         insts[i] = m.inst;
     }
@@ -540,8 +584,8 @@ int build_tables(cfd_batch* b) {
                 g.dir = dir;
                 g.shape = f64 ? (dir == DIR_X ? 0 : kMarchShape) : b->shape[model][dir];
                 g.offset = (int)all.size();
-                const Shape sh = dir == DIR_X ? kShapesX[f64 ? 0 : g.shape] : shape_y[model][f64];
-                g.rows = sh.ts;
+                const Shape sh = dir == DIR_X ? shape_x[model][f64] : shape_y[model][f64];
+                g.rows = dir == DIR_X ? sh.na : sh.ts;
                 for (int idx : order) {
                     const Member& m = b->members[idx];
                     // finished members have no tiles
@@ -992,6 +1036,15 @@ int cfd_batch_get_march_rows(cfd_batch* b, int model, int* rows) {
     if (!b || model < 0 || model > 1 || !rows) return cfd_fail(CFD_ERR_INVALID, "bad arguments");
     if (int r = build_tables(b)) return r;
     *rows = b->march_used[model];
+    return CFD_OK;
+}
+
+int cfd_batch_get_segment_rows(cfd_batch* b, int model, int precision, int* rows) {
+    if (!b || model < 0 || model > 1 || !rows ||
+        (precision != CFD_PREC_MIXED && precision != CFD_PREC_FP64_FAST))
+        return cfd_fail(CFD_ERR_INVALID, "bad arguments");
+    if (int r = build_tables(b)) return r;
+    *rows = b->seg_used[model][precision == CFD_PREC_FP64_FAST];
     return CFD_OK;
 }
 

@@ -723,7 +723,7 @@ __global__ void __launch_bounds__(128, MODEL == MODEL_EULER ? 4 : 2) fast_march_
 // ---- x sweep by warp segments -----------------------------------------------
 // The 32 lanes hold 32 consecutive cells of a row (kSegCells outputs and a
 // 2-cell halo at each end); neighbour values come from the adjacent lanes by
-// shuffles.  A warp walks the kSegRows rows of its tile.
+// shuffles.  A warp walks the rows of its tile (A.rows, chosen per launch).
 template <int N>
 __device__ __forceinline__ void shfl_up64(const double* x, double* y) {
 #pragma unroll
@@ -764,7 +764,7 @@ __device__ __forceinline__ void segment64_tile(const MixedArgs& A, const TileGeo
     }
     src = min(max(src, 0), nx - 1);
     const bool writer = lane >= 2 && lane < 2 + mixed::kSegCells && ga < nx;
-    const int row_end = min(g.b_org + mixed::kSegRows, ny);
+    const int row_end = min(g.b_org + A.rows, ny);
 
     double nh[NV];
     load64<MODEL>(pin, g.b_org * pitch + src, nh);

@@ -116,7 +116,7 @@ __device__ __forceinline__ void march_finish(DevState* st, const double* partial
 // 128 instead of 163 registers, 4 instead of 3 CTAs per SM, measured 7 %
 // faster (Euler measured 24 % slower that way).
 template <int MODEL>
-constexpr bool march_win_smem() {
+__host__ __device__ constexpr bool march_win_smem() {
     return MODEL == MODEL_ALLAIRE;
 }
 
@@ -475,14 +475,16 @@ __global__ void __launch_bounds__(128) mixed_march_kernel(MixedArgs A) {
 }
 
 // ---- x sweep by warp segments ------------------------------------------------
-// A warp owns a tile of kSegCells columns x kSegRows rows and walks its rows:
+// A warp owns a tile of kSegCells columns x A.rows rows and walks its rows:
 // the 32 lanes hold 32 consecutive cells of a row (kSegCells outputs plus a
 // 2-cell halo at each end), so every load and store is coalesced, and the
 // neighbours each stencil step needs (primitive states, face states, fluxes)
 // come from the adjacent lanes by warp shuffles: no shared memory, no
 // barrier.  The arithmetic is the tiled sweep's, in the same order.
 constexpr int kSegCells = 28;  // outputs per row segment
-constexpr int kSegRows = 32;   // rows of a tile
+// rows of a tile: chosen per launch on the host (kSegMinRows..kSegRows) so
+// that the tiles fill the resident warps
+constexpr int kSegRows = 32, kSegMinRows = 12;
 
 template <int N>
 __device__ __forceinline__ void shfl_up_n(const float* x, float* y) {
@@ -522,7 +524,7 @@ __device__ __forceinline__ void segment_tile(const MixedArgs& A, const TileGeom&
     }
     src = min(max(src, 0), nx - 1);
     const bool writer = lane >= 2 && lane < 2 + kSegCells && ga < nx;
-    const int row_end = min(g.b_org + kSegRows, ny);
+    const int row_end = min(g.b_org + A.rows, ny);
 
     float nh[NV], nl[NV];
     load_cell<MODEL>(I, bin, (long long)g.b_org * I.pitch + src, nh, nl);

@@ -308,6 +308,12 @@ int cfd_batch_get_shapes(cfd_batch* b, int model, int* shape_x, int* shape_y);
  * march or the model has no active member).  Results do not depend on it. */
 int cfd_batch_set_march_rows(cfd_batch* b, int model, int rows);
 int cfd_batch_get_march_rows(cfd_batch* b, int model, int* rows);
+/* Rows of the x sweep's warp-segment tiles (28 columns each) in the current
+ * tile list of a model and form (precision CFD_PREC_MIXED or
+ * CFD_PREC_FP64_FAST): in [12, 32], chosen for every tile list so that the
+ * tiles fill the resident warps; 0 when that model and form have no active
+ * member.  Results do not depend on it. */
+int cfd_batch_get_segment_rows(cfd_batch* b, int model, int precision, int* rows);
 int cfd_batch_status(cfd_batch* b, int id, cfd_status* st);
 /* ids, steps taken, done flags and times of all members (cap entries). */
 int cfd_batch_poll(cfd_batch* b, int cap, int* ids, int* steps, int* done, double* t, int* count);

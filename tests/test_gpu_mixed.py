@@ -152,6 +152,35 @@ def test_tile_shapes_do_not_change_results():
             assert np.array_equal(outs[0][k], o[k])
 
 
+@pytest.mark.parametrize("prec", [G.MIXED, G.FP64_FAST])
+def test_segment_rows_do_not_change_results(prec):
+    """The x segments' row count is chosen per tile list (a lone small grid
+    gets short tiles so that they fill the resident warps, a full batch
+    longer ones); a member's result is the same bits either way."""
+    cfg = G.recipe_config("water_shock_air_bubble", 300, 200)
+    cfg.precision = prec
+    ic = G.recipe_ic(cfg, "water_shock_air_bubble")
+    big = G.recipe_config("water_shock_air_bubble", 2048, 1024)
+    big.precision = prec
+    big_ic = G.recipe_ic(big, "water_shock_air_bubble")
+    with G.Batch() as b:
+        i = b.add(cfg, ic, 25)
+        alone_rows = b.segment_rows(G.ALLAIRE, prec)
+        assert b.segment_rows(G.EULER, prec) == 0  # no Euler member
+        b.step(25)
+        alone = b.download(i)
+    with G.Batch() as b:
+        b.add(big, big_ic, 25)
+        b.add(big, big_ic, 25)
+        i = b.add(cfg, ic, 25)
+        mix_rows = b.segment_rows(G.ALLAIRE, prec)
+        b.step(25)
+        in_mix = b.download(i)
+    print(f"precision {prec}: segment rows alone {alone_rows}, in the mix {mix_rows}")
+    assert 12 <= alone_rows < mix_rows <= 32
+    assert np.array_equal(alone, in_mix)
+
+
 def test_march_strip_lengths_do_not_change_results():
     """Marching strips of any length (the automatic choice, the shortest, an
     odd one that leaves ragged last strips, the longest) give the tiles' bits;
