@@ -476,10 +476,11 @@ __device__ __forceinline__ void speeds(const DPar& P, const double* N, double& s
 // Rows staged ahead through shared memory: a lane copies the cells of rows
 // k+1 .. k+kAhead of its column global -> shared with cp.async while it
 // computes row k, so no registers are held by the loads in flight.  A ring
-// of kAhead + 1 slots, so the slot refilled at row k is the one read at row
-// k - 1; per slot NU 16-byte units per lane (components 0-1, 2-3, and for
-// Allaire E and z), lane-major.
-constexpr int kAhead = 3, kSlots = kAhead + 1;
+// of kAhead + 2 slots: the slot refilled at row k is the one read at row
+// k - 2, so row k - 1 is still there when row k computes (its update starts
+// from it, and it is not carried in registers); per slot NU 16-byte units
+// per lane (components 0-1, 2-3, and for Allaire E and z), lane-major.
+constexpr int kAhead = 3, kSlots = kAhead + 2;
 template <int MODEL>
 __host__ __device__ constexpr int stage_units() {
     return MODEL == MODEL_ALLAIRE ? 3 : 2;
@@ -527,8 +528,9 @@ __device__ __forceinline__ void stage_read(const char* stg, int s, double* U) {
 // and face states of row k - 1, the flux at the face between rows k - 2 and
 // k - 1, and the update of row k - 2.  Carried from row to row: the
 // primitive states of rows k - 1 and k - 2 (and 1/rho, 1/eps of row k - 1),
-// the evolved high-face state of row k - 2, the raw state of row k - 1 and
-// the partly updated state of row k - 2 (its low-face flux applied).
+// the evolved high-face state of row k - 2 and the partly updated state of
+// row k - 2 (its low-face flux applied); the raw state of row k - 1 is read
+// again from its staging slot.
 template <int MODEL>
 __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom& g) {
     using MT = ModelTraits<MODEL>;
@@ -568,13 +570,13 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
     };
 
     Prim64<MODEL> Q1, Q2;          // rows k-1, k-2
-    double H1[NV], A2[NV], Pp[NV]; // raw row k-1, partly updated row k-2, high face of row k-2
+    double A2[NV], Pp[NV];         // partly updated row k-2, high face of row k-2
     unsigned flp = 0;
     double usL = 0.0, zsL = 0.0;   // u*, z* at the low face of row k-2
     double z3 = 0.0;               // z of row k-3 (upwind z update)
     double rmu = 0.0, rmv = 0.0, rm1 = 0.0, rm2 = 0.0;
 #pragma unroll
-    for (int q = 0; q < NV; ++q) Q1.W[q] = Q2.W[q] = H1[q] = A2[q] = Pp[q] = 0.0;
+    for (int q = 0; q < NV; ++q) Q1.W[q] = Q2.W[q] = A2[q] = Pp[q] = 0.0;
     Q1.r = Q1.ie = Q1.kn = Q2.r = Q2.ie = Q2.kn = 0.0;
 
     // this lane's staging slots; rows r0-2 .. r0-3+kAhead in flight first
@@ -594,10 +596,11 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
         src_row(k, neg);
         cp_async_wait<kAhead - 1>();  // row k has arrived
         stage_read<MODEL>(stg, slot, h);
-        const int refill = slot == 0 ? kSlots - 1 : slot - 1;  // read at row k - 1
+        const int refill = slot >= 2 ? slot - 2 : slot + kSlots - 2;  // read at row k - 2
         if (k + kAhead <= r1 + 1)
             stage_issue<MODEL>(stg, refill, pin, src_row(k + kAhead, dummy) * pitch + c);
         mixed::cp_async_commit();
+        const int slot1 = slot == 0 ? kSlots - 1 : slot - 1;  // row k - 1
         slot = slot == kSlots - 1 ? 0 : slot + 1;
         // sweep frame: mirror sign, then (u, v) -> (v, -u) (E/sourcecode/euler_colsweep.cpp:22-29)
         {
@@ -662,7 +665,15 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
                     rm2 += m2;
                 }
             }
-            // row k-1 takes the flux at its low face
+            // row k-1 takes the flux at its low face (it is updated only
+            // when inside the strip, so never a mirrored row)
+            double H1[NV];
+            stage_read<MODEL>(stg, slot1, H1);
+            {
+                const double m = H1[MT::IM];
+                H1[MT::IM] = H1[MT::IT];
+                H1[MT::IT] = -m;
+            }
 #pragma unroll
             for (int q = 0; q < NV; ++q) A2[q] = fma(k_upd, F[q], H1[q]);
             if constexpr (MODEL == MODEL_ALLAIRE) {
@@ -677,10 +688,7 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
         Q2 = Q1;
         Q1 = Q0;
 #pragma unroll
-        for (int q = 0; q < NV; ++q) {
-            Pp[q] = Pn[q];
-            H1[q] = h[q];
-        }
+        for (int q = 0; q < NV; ++q) Pp[q] = Pn[q];
         flp = fln;
     }
 

@@ -3,11 +3,11 @@
 // Marching strips (the y sweep): a warp owns a strip of 32 lines x A.rows
 // cells along the sweep of one instance: lane = line, and every lane walks
 // along its line one cell at a time, carrying the window the stencil needs
-// from one row to the next (primitive states, face states, raw cells, flux;
-// in registers, or for the six-component Allaire model partly in a per-lane
-// column of shared memory).  The rows ahead of the one being computed are
-// copied global -> shared with cp.async, three rows in flight, so no
-// registers are held by the loads.  The strip length is chosen per launch on the
+// from one row to the next in registers (primitive states, the face state,
+// the flux).  The rows ahead of the one being computed are copied global ->
+// shared with cp.async, three rows in flight, so no registers are held by
+// the loads, and each row stays in shared memory until the update that
+// starts from it.  The strip length is chosen per launch on the
 // host (kMarchMinRows..kMarchMaxRows) so that the strips fill the resident
 // warps.  No barrier is needed, and only the two halo cells at each end of
 // a strip are re-read.  In the y sweep the lanes are 32 consecutive columns,
@@ -107,116 +107,28 @@ __device__ __forceinline__ void march_finish(DevState* st, const double* partial
     }
 }
 
-// The part of a lane's window carried from one row to the next: the raw
-// cells of rows k-1 and k-2 in the sweep frame (the update of row k-2 starts
-// from them; a reload from global memory measured 5 % slower), the state at
-// the high face of row k-2 and the flux at its low face.  Euler keeps it in
-// registers.  Allaire (six components) keeps it in shared memory, entry-major
-// with one column per lane (no bank conflicts, no lane reads another's):
-// 128 instead of 163 registers, 4 instead of 3 CTAs per SM, measured 7 %
-// faster (Euler measured 24 % slower that way).
-template <int MODEL>
-__host__ __device__ constexpr bool march_win_smem() {
-    return MODEL == MODEL_ALLAIRE;
-}
-
-// Rows staged ahead through shared memory with cp.async (no registers held
-// by the loads in flight): a ring of kMSlots slots, kMAhead rows in flight,
-// per slot MU 16-byte units per lane (value and compensation words of
-// components 0-3; for Allaire E and z with their compensation words).
-constexpr int kMAhead = 3, kMSlots = kMAhead + 1;
+// Rows staged through shared memory with cp.async (no registers held by the
+// loads in flight): a ring of kMSlots slots per lane holding rows k-2 .. k+3
+// while row k is computed; kMAhead rows in flight, row k + kMAhead issued
+// into the slot of row k - 3 once row k has arrived; per slot MU 16-byte
+// units per lane (value and compensation words of components 0-3; for
+// Allaire E and z with their compensation words).  The raw cells of rows
+// k-1 and k-2 that the update of row k-2 starts from are therefore read
+// again from the ring rather than carried in registers: 124 -> 115
+// registers for Euler and 5 % less time per y sweep; Allaire's carried
+// window (face state, flux) then fits in its 128 registers, where it had
+// to sit in shared memory before.
+constexpr int kMAhead = 3, kMSlots = kMAhead + 3;
 template <int MODEL>
 __host__ __device__ constexpr int march_units() {
     return MODEL == MODEL_ALLAIRE ? 3 : 2;
 }
 
-// Dynamic shared memory of a 4-warp marching CTA: the carried window
-// (Allaire), then the staging ring.
-template <int MODEL>
-__host__ __device__ constexpr int march_win_bytes() {
-    return march_win_smem<MODEL>() ? 4 * 8 * ModelTraits<MODEL>::NV * 32 * (int)sizeof(float) : 0;
-}
+// Dynamic shared memory of a 4-warp marching CTA: the staging rings.
 template <int MODEL>
 __host__ __device__ constexpr int march_smem_bytes() {
-    return march_win_bytes<MODEL>() + 4 * kMSlots * march_units<MODEL>() * 32 * 16;
+    return 4 * kMSlots * march_units<MODEL>() * 32 * 16;
 }
-
-template <int MODEL, bool SMEM = march_win_smem<MODEL>()>
-struct MarchWin;
-
-template <int MODEL>
-struct MarchWin<MODEL, false> {
-    static constexpr int NV = ModelTraits<MODEL>::NV;
-    float H0[NV], L0[NV], H1[NV], L1[NV], H2[NV], L2[NV], Pp[NV], Fl[NV];
-    __device__ __forceinline__ void init(int) {
-#pragma unroll
-        for (int q = 0; q < NV; ++q) H1[q] = L1[q] = H2[q] = L2[q] = Pp[q] = Fl[q] = 0.f;
-    }
-    // raw cell of row k (the current row)
-    __device__ __forceinline__ void put_raw(const float* h, const float* l) {
-#pragma unroll
-        for (int q = 0; q < NV; ++q) {
-            H0[q] = h[q];
-            L0[q] = l[q];
-        }
-    }
-    // raw cell of row k-2
-    __device__ __forceinline__ void get_raw2(float* h, float* l) const {
-#pragma unroll
-        for (int q = 0; q < NV; ++q) {
-            h[q] = H2[q];
-            l[q] = L2[q];
-        }
-    }
-    __device__ __forceinline__ float& face(int q) { return Pp[q]; }
-    __device__ __forceinline__ float& flux(int q) { return Fl[q]; }
-    // row k becomes row k-1
-    __device__ __forceinline__ void advance() {
-#pragma unroll
-        for (int q = 0; q < NV; ++q) {
-            H2[q] = H1[q];
-            L2[q] = L1[q];
-            H1[q] = H0[q];
-            L1[q] = L0[q];
-        }
-    }
-};
-
-template <int MODEL>
-struct MarchWin<MODEL, true> {
-    static constexpr int NV = ModelTraits<MODEL>::NV;
-    // per warp 8 x NV entries of 32 floats: raw cells of the last three rows
-    // (a ring: value and compensation), the face state, the flux
-    float* wb;
-    int ws;  // ring slot of row k
-    __device__ __forceinline__ void init(int lane) {
-        extern __shared__ float march_win[];
-        wb = march_win + (threadIdx.x >> 5) * (8 * NV * 32) + lane;
-        ws = 0;
-#pragma unroll
-        for (int q = 0; q < NV; ++q) face(q) = flux(q) = 0.f;
-    }
-    __device__ __forceinline__ float& rh(int sl, int q) { return wb[(sl * 2 * NV + q) * 32]; }
-    __device__ __forceinline__ float& rl(int sl, int q) { return wb[(sl * 2 * NV + NV + q) * 32]; }
-    __device__ __forceinline__ void put_raw(const float* h, const float* l) {
-#pragma unroll
-        for (int q = 0; q < NV; ++q) {
-            rh(ws, q) = h[q];
-            rl(ws, q) = l[q];
-        }
-    }
-    __device__ __forceinline__ void get_raw2(float* h, float* l) {
-        const int rs = ws == 2 ? 0 : ws + 1;  // ring slot of row k-2
-#pragma unroll
-        for (int q = 0; q < NV; ++q) {
-            h[q] = rh(rs, q);
-            l[q] = rl(rs, q);
-        }
-    }
-    __device__ __forceinline__ float& face(int q) { return wb[(6 * NV + q) * 32]; }
-    __device__ __forceinline__ float& flux(int q) { return wb[(7 * NV + q) * 32]; }
-    __device__ __forceinline__ void advance() { ws = ws == 2 ? 0 : ws + 1; }
-};
 
 // One strip: cells [r0, r1) along the sweep of lines [b_org, b_org + 32) of
 // instance g.inst ("row" below means a position along the sweep).
@@ -261,19 +173,18 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
 
     float W1[NV], W2[NV];       // W(k-1), W(k-2)
     unsigned flp = 0;           // physicality flags of row k-2
-    MarchWin<MODEL> win;        // raw cells, face state and flux carried along
-    win.init(lane);
+    float Pp[NV], Fl[NV];       // state at the high face of row k-2, flux at its low face
     float us_low = 0.f, zs_low = 0.f;
     float z3 = 0.f;             // z of row k-3 (first-order z update)
     float rmu = 0.f, rmv = 0.f;
     double rm1 = 0.0, rm2 = 0.0;
 #pragma unroll
-    for (int q = 0; q < NV; ++q) W1[q] = W2[q] = 0.f;
+    for (int q = 0; q < NV; ++q) W1[q] = W2[q] = Pp[q] = Fl[q] = 0.f;
 
     // rows staged ahead (y sweep: line = column, along = row)
     extern __shared__ __align__(16) char march_stage[];
     constexpr int MU = march_units<MODEL>();
-    char* stg = march_stage + march_win_bytes<MODEL>() + (threadIdx.x >> 5) * (kMSlots * MU * 32 * 16) +
+    char* stg = march_stage + (threadIdx.x >> 5) * (kMSlots * MU * 32 * 16) +
                 16 * lane;
     auto issue = [&](int s, int k) {
         bool ng;
@@ -283,6 +194,18 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
         if constexpr (MODEL == MODEL_ALLAIRE) {
             cp_async8(stg + ((s * MU + 2) * 32) * 16, I.q2[bin][0] + off);
             cp_async8(stg + ((s * MU + 2) * 32) * 16 + 8, I.q2[bin][1] + off);
+        }
+    };
+    // the raw cell staged in slot s (as stored: no mirror, no rotation)
+    auto staged = [&](int s, float* h, float* l) {
+        const float4 a = *reinterpret_cast<const float4*>(stg + ((s * MU + 0) * 32) * 16);
+        const float4 b = *reinterpret_cast<const float4*>(stg + ((s * MU + 1) * 32) * 16);
+        h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w;
+        l[0] = b.x; l[1] = b.y; l[2] = b.z; l[3] = b.w;
+        if constexpr (MODEL == MODEL_ALLAIRE) {
+            const float4 e = *reinterpret_cast<const float4*>(stg + ((s * MU + 2) * 32) * 16);
+            h[4] = e.x; h[5] = e.y;
+            l[4] = e.z; l[5] = e.w;
         }
     };
 #pragma unroll
@@ -297,22 +220,13 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
         bool neg;
         src_row(k, neg);
         asm volatile("cp.async.wait_group %0;\n" ::"n"(kMAhead - 1) : "memory");
-        {
-            const float4 a = *reinterpret_cast<const float4*>(stg + ((slot * MU + 0) * 32) * 16);
-            const float4 b = *reinterpret_cast<const float4*>(stg + ((slot * MU + 1) * 32) * 16);
-            h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w;
-            l[0] = b.x; l[1] = b.y; l[2] = b.z; l[3] = b.w;
-            if constexpr (MODEL == MODEL_ALLAIRE) {
-                const float4 e = *reinterpret_cast<const float4*>(stg + ((slot * MU + 2) * 32) * 16);
-                h[4] = e.x; h[5] = e.y;
-                l[4] = e.z; l[5] = e.w;
-            }
-        }
-        if (k + kMAhead <= r1 + 1) issue(slot == 0 ? kMSlots - 1 : slot - 1, k + kMAhead);
+        staged(slot, h, l);
+        // row k + kMAhead into the slot of row k - 3 (read three rows ago)
+        if (k + kMAhead <= r1 + 1) issue(slot >= 3 ? slot - 3 : slot + kMSlots - 3, k + kMAhead);
         cp_async_commit();
+        const int slot2 = slot >= 2 ? slot - 2 : slot + kMSlots - 2;  // row k - 2
         slot = slot == kMSlots - 1 ? 0 : slot + 1;
         march_frame_in<MODEL, DIR>(h, l, neg);
-        win.put_raw(h, l);
         float W0[NV];
         c2p_mixed<MODEL>(I, P, h, l, W0);
 
@@ -344,7 +258,7 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
             const bool second = !god && (flp & 1u) && (fln & 2u) && (flp & 4u) && (fln & 8u);
 #pragma unroll
             for (int q = 0; q < NV; ++q) {
-                WL[q] = second ? win.face(q) : W2[q];
+                WL[q] = second ? Pp[q] : W2[q];
                 WR[q] = second ? Mn[q] : W1[q];
             }
             hllc_prim<MODEL>(P, WL, WR, Fh);
@@ -354,11 +268,12 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
         if (k >= r0 + 2) {
             const int row = k - 2;  // inside [r0, r1): no mirror, no sign
             float hh[NV], ll[NV];
-            win.get_raw2(hh, ll);  // row k-2 as loaded, in the sweep frame
+            staged(slot2, hh, ll);  // row k-2 as loaded (inside: no mirror)
+            march_frame_in<MODEL, DIR>(hh, ll, false);
 #pragma unroll
             for (int q = 0; q < NV; ++q) {
                 if (MODEL == MODEL_ALLAIRE && q == 5) continue;
-                comp_add(hh[q], ll[q], k_upd * (win.flux(q) - Fh[q]));
+                comp_add(hh[q], ll[q], k_upd * (Fl[q] - Fh[q]));
             }
             if constexpr (MODEL == MODEL_ALLAIRE) {
                 const float usL = us_low, usR = Fh[NV], zsL = zs_low, zsR = Fh[NV + 1];
@@ -422,16 +337,15 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
         for (int q = 0; q < NV; ++q) {
             W2[q] = W1[q];
             W1[q] = W0[q];
-            win.face(q) = Pn[q];
+            Pp[q] = Pn[q];
         }
         flp = fln;
         if (k >= r0 + 1) {
 #pragma unroll
-            for (int q = 0; q < NV; ++q) win.flux(q) = Fh[q];
+            for (int q = 0; q < NV; ++q) Fl[q] = Fh[q];
             us_low = Fh[NV];
             zs_low = MODEL == MODEL_ALLAIRE ? Fh[NV + 1] : 0.f;
         }
-        win.advance();
     }
 
     if (DIR == DIR_X) return;  // the y sweep reduces
