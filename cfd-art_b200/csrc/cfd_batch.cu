@@ -119,8 +119,8 @@ template <int MODEL>
 int segment_per_sm() {
     static int per_sm = 0;
     if (!per_sm) {
-        cudaError_t e =
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_segment_x_kernel<MODEL>, 128, 0);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, mixed_segment_x_kernel<MODEL>, 128, seg_smem_bytes<MODEL>());
         if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     }
     return per_sm;
@@ -129,7 +129,7 @@ int segment_per_sm() {
 template <int MODEL>
 int launch_segment(const MixedArgs& a, int sms, cudaStream_t st) {
     const int warps = std::max(1, std::min(a.ntiles, segment_per_sm<MODEL>() * sms * 4));
-    mixed_segment_x_kernel<MODEL><<<(warps + 3) / 4, 128, 0, st>>>(a);
+    mixed_segment_x_kernel<MODEL><<<(warps + 3) / 4, 128, seg_smem_bytes<MODEL>(), st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cfd_fail(CFD_ERR_CUDA, "segment launch: %s", cudaGetErrorString(e));
     return CFD_OK;
@@ -153,7 +153,7 @@ int segment64_per_sm() {
     static int per_sm = 0;
     if (!per_sm) {
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per_sm, fast::fast_segment_x_kernel<MODEL>, 128, 0);
+            &per_sm, fast::fast_segment_x_kernel<MODEL>, 128, fast::segment64_smem_bytes<MODEL>());
         if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     }
     return per_sm;
@@ -164,7 +164,7 @@ int launch_fast(int dir, const MixedArgs& a, int sms, cudaStream_t st) {
     const int per_sm = dir == DIR_X ? segment64_per_sm<MODEL>() : march64_per_sm<MODEL>();
     const int warps = std::max(1, std::min(a.ntiles, per_sm * sms * 4));
     if (dir == DIR_X)
-        fast::fast_segment_x_kernel<MODEL><<<(warps + 3) / 4, 128, 0, st>>>(a);
+        fast::fast_segment_x_kernel<MODEL><<<(warps + 3) / 4, 128, fast::segment64_smem_bytes<MODEL>(), st>>>(a);
     else
         fast::fast_march_kernel<MODEL><<<(warps + 3) / 4, 128, fast::march64_smem_bytes<MODEL>(), st>>>(a);
     cudaError_t e = cudaGetLastError();

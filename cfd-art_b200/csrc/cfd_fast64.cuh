@@ -475,19 +475,30 @@ __device__ __forceinline__ void speeds(const DPar& P, const double* N, double& s
 
 // Rows staged ahead through shared memory: a lane copies the cells of rows
 // k+1 .. k+kAhead of its column global -> shared with cp.async while it
-// computes row k, so no registers are held by the loads in flight.  A ring
-// of kAhead + 2 slots: the slot refilled at row k is the one read at row
-// k - 2, so row k - 1 is still there when row k computes (its update starts
-// from it, and it is not carried in registers); per slot NU 16-byte units
-// per lane (components 0-1, 2-3, and for Allaire E and z), lane-major.
-constexpr int kAhead = 3, kSlots = kAhead + 2;
+// computes row k, so no registers are held by the loads in flight; per slot
+// NU 16-byte units per lane (components 0-1, 2-3, and for Allaire E and z),
+// lane-major.  Euler's ring has kAhead + 2 slots: the slot refilled at row k
+// is the one read at row k - 2, so row k - 1 is still there when row k
+// computes and its update starts from it there rather than from registers
+// (8 fewer registers, y sweep 0.448 -> 0.421 ms at 4096^2).  Allaire, 2 CTAs
+// per SM either way, measured 1.5 % slower like that; it carries row k - 1
+// in registers and refills the slot read at row k - 1 (kAhead + 1 slots).
+constexpr int kAhead = 3;
+template <int MODEL>
+__host__ __device__ constexpr bool march64_reread() {
+    return MODEL == MODEL_EULER;
+}
+template <int MODEL>
+__host__ __device__ constexpr int march64_slots() {
+    return kAhead + (march64_reread<MODEL>() ? 2 : 1);
+}
 template <int MODEL>
 __host__ __device__ constexpr int stage_units() {
     return MODEL == MODEL_ALLAIRE ? 3 : 2;
 }
 template <int MODEL>
 __host__ __device__ constexpr int march64_smem_bytes() {
-    return 4 * kSlots * stage_units<MODEL>() * 32 * 16;  // 4 warps per CTA
+    return 4 * march64_slots<MODEL>() * stage_units<MODEL>() * 32 * 16;  // 4 warps per CTA
 }
 
 template <int N>
@@ -530,7 +541,7 @@ __device__ __forceinline__ void stage_read(const char* stg, int s, double* U) {
 // primitive states of rows k - 1 and k - 2 (and 1/rho, 1/eps of row k - 1),
 // the evolved high-face state of row k - 2 and the partly updated state of
 // row k - 2 (its low-face flux applied); the raw state of row k - 1 is read
-// again from its staging slot.
+// again from its staging slot (Euler) or carried (Allaire).
 template <int MODEL>
 __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom& g) {
     using MT = ModelTraits<MODEL>;
@@ -581,7 +592,12 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
 
     // this lane's staging slots; rows r0-2 .. r0-3+kAhead in flight first
     extern __shared__ __align__(16) char fast_stage[];
-    char* stg = fast_stage + (threadIdx.x >> 5) * (kSlots * stage_units<MODEL>() * 32 * 16) + 16 * lane;
+    constexpr bool reread = march64_reread<MODEL>();
+    constexpr int NS = march64_slots<MODEL>();
+    double H1c[NV];  // raw row k-1 in the sweep frame (when carried)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) H1c[q] = 0.0;
+    char* stg = fast_stage + (threadIdx.x >> 5) * (NS * stage_units<MODEL>() * 32 * 16) + 16 * lane;
     bool dummy;
 #pragma unroll
     for (int j = 0; j < kAhead; ++j) {
@@ -596,12 +612,12 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
         src_row(k, neg);
         cp_async_wait<kAhead - 1>();  // row k has arrived
         stage_read<MODEL>(stg, slot, h);
-        const int refill = slot >= 2 ? slot - 2 : slot + kSlots - 2;  // read at row k - 2
+        const int slot1 = slot == 0 ? NS - 1 : slot - 1;                   // row k - 1
+        const int refill = !reread ? slot1 : slot >= 2 ? slot - 2 : slot + NS - 2;  // row k - 1 or k - 2
         if (k + kAhead <= r1 + 1)
             stage_issue<MODEL>(stg, refill, pin, src_row(k + kAhead, dummy) * pitch + c);
         mixed::cp_async_commit();
-        const int slot1 = slot == 0 ? kSlots - 1 : slot - 1;  // row k - 1
-        slot = slot == kSlots - 1 ? 0 : slot + 1;
+        slot = slot == NS - 1 ? 0 : slot + 1;
         // sweep frame: mirror sign, then (u, v) -> (v, -u) (E/sourcecode/euler_colsweep.cpp:22-29)
         {
             const double m = h[MT::IM], n = neg ? -h[MT::IT] : h[MT::IT];
@@ -668,11 +684,14 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
             // row k-1 takes the flux at its low face (it is updated only
             // when inside the strip, so never a mirrored row)
             double H1[NV];
-            stage_read<MODEL>(stg, slot1, H1);
-            {
+            if constexpr (reread) {
+                stage_read<MODEL>(stg, slot1, H1);
                 const double m = H1[MT::IM];
                 H1[MT::IM] = H1[MT::IT];
                 H1[MT::IT] = -m;
+            } else {
+#pragma unroll
+                for (int q = 0; q < NV; ++q) H1[q] = H1c[q];
             }
 #pragma unroll
             for (int q = 0; q < NV; ++q) A2[q] = fma(k_upd, F[q], H1[q]);
@@ -688,7 +707,10 @@ __device__ __forceinline__ void march64_strip(const MixedArgs& A, const TileGeom
         Q2 = Q1;
         Q1 = Q0;
 #pragma unroll
-        for (int q = 0; q < NV; ++q) Pp[q] = Pn[q];
+        for (int q = 0; q < NV; ++q) {
+            Pp[q] = Pn[q];
+            if constexpr (!reread) H1c[q] = h[q];
+        }
         flp = fln;
     }
 
@@ -743,6 +765,12 @@ __device__ __forceinline__ void shfl_down64(const double* x, double* y) {
     for (int q = 0; q < N; ++q) y[q] = __shfl_down_sync(0xffffffffu, x[q], 1);
 }
 
+constexpr int kSegSlots = kAhead + 1;
+template <int MODEL>
+__host__ __device__ constexpr int segment64_smem_bytes() {
+    return 4 * kSegSlots * stage_units<MODEL>() * 32 * 16;  // 4 warps per CTA
+}
+
 template <int MODEL>
 __device__ __forceinline__ void segment64_tile(const MixedArgs& A, const TileGeom& g) {
     using MT = ModelTraits<MODEL>;
@@ -774,13 +802,23 @@ __device__ __forceinline__ void segment64_tile(const MixedArgs& A, const TileGeo
     const bool writer = lane >= 2 && lane < 2 + mixed::kSegCells && ga < nx;
     const int row_end = min(g.b_org + A.rows, ny);
 
-    double nh[NV];
-    load64<MODEL>(pin, g.b_org * pitch + src, nh);
+    // rows staged kAhead ahead, the slot refilled at row r the one read at row r - 1
+    extern __shared__ __align__(16) char seg64_stage[];
+    char* stg = seg64_stage + (threadIdx.x >> 5) * (kSegSlots * stage_units<MODEL>() * 32 * 16) + 16 * lane;
+#pragma unroll
+    for (int j = 0; j < kAhead; ++j) {
+        if (g.b_org + j < row_end) stage_issue<MODEL>(stg, j, pin, (g.b_org + j) * pitch + src);
+        mixed::cp_async_commit();
+    }
+    int slot = 0;
     for (int row = g.b_org; row < row_end; ++row) {
         double h[NV];
-#pragma unroll
-        for (int q = 0; q < NV; ++q) h[q] = nh[q];
-        if (row + 1 < row_end) load64<MODEL>(pin, (row + 1) * pitch + src, nh);
+        cp_async_wait<kAhead - 1>();  // row `row` has arrived
+        stage_read<MODEL>(stg, slot, h);
+        if (row + kAhead < row_end)
+            stage_issue<MODEL>(stg, slot == 0 ? kSegSlots - 1 : slot - 1, pin, (row + kAhead) * pitch + src);
+        mixed::cp_async_commit();
+        slot = slot == kSegSlots - 1 ? 0 : slot + 1;
         if (neg) h[MT::IM] = -h[MT::IM];
         Prim64<MODEL> Q;
         c2p<MODEL>(P, h, Q);
@@ -831,8 +869,9 @@ __device__ __forceinline__ void segment64_tile(const MixedArgs& A, const TileGeo
     }
 }
 
-// At least 4 CTAs per SM: Allaire bounded from 144 to 128 registers (24 bytes
-// spill) measured 25 % faster than at 3 CTAs; Euler (96 registers) runs 5.
+// At least 4 CTAs per SM: Allaire bounded to 128 registers measured 25 %
+// faster than at the 3 CTAs of its unbounded count; Euler (96 registers)
+// runs 5.
 template <int MODEL>
 __global__ void __launch_bounds__(128, 4) fast_segment_x_kernel(MixedArgs A) {
     const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);

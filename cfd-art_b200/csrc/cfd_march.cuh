@@ -35,15 +35,6 @@ namespace mixed {
 
 constexpr int kMarchMaxRows = 64, kMarchMinRows = 16;  // rows of a strip (its width is one warp)
 
-// Raw (unrotated) cell of buffer `buf` at position `along` of line `line`.
-template <int MODEL, int DIR>
-__device__ __forceinline__ void march_load(const Inst& I, int buf, int along, int line, float* h,
-                                           float* l) {
-    const long long off = DIR == DIR_Y ? (long long)along * I.pitch + line
-                                       : (long long)line * I.pitch + along;
-    load_cell<MODEL>(I, buf, off, h, l);
-}
-
 // y-sweep frame: the boundary sign of a mirrored row, then (u, v) -> (v, -u).
 template <int MODEL>
 __device__ __forceinline__ void march_rotate_in(float* h, float* l, bool neg) {
@@ -130,6 +121,34 @@ __host__ __device__ constexpr int march_smem_bytes() {
     return 4 * kMSlots * march_units<MODEL>() * 32 * 16;
 }
 
+// Starts copying the cell at element offset `off` of buffer `buf` (value and
+// compensation words) into slot `s` of this lane's staging ring `stg`.
+template <int MODEL>
+__device__ __forceinline__ void mstage_issue(char* stg, int s, const MPlanes& Q, long long off) {
+    constexpr int MU = march_units<MODEL>();
+    cp_async16(stg + ((s * MU + 0) * 32) * 16, Q.v4 + off);
+    cp_async16(stg + ((s * MU + 1) * 32) * 16, Q.c4 + off);
+    if constexpr (MODEL == MODEL_ALLAIRE) {
+        cp_async8(stg + ((s * MU + 2) * 32) * 16, Q.v2 + off);
+        cp_async8(stg + ((s * MU + 2) * 32) * 16 + 8, Q.c2 + off);
+    }
+}
+
+// The cell staged in slot `s` (as stored: no mirror, no rotation).
+template <int MODEL>
+__device__ __forceinline__ void mstage_read(const char* stg, int s, float* h, float* l) {
+    constexpr int MU = march_units<MODEL>();
+    const float4 a = *reinterpret_cast<const float4*>(stg + ((s * MU + 0) * 32) * 16);
+    const float4 b = *reinterpret_cast<const float4*>(stg + ((s * MU + 1) * 32) * 16);
+    h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w;
+    l[0] = b.x; l[1] = b.y; l[2] = b.z; l[3] = b.w;
+    if constexpr (MODEL == MODEL_ALLAIRE) {
+        const float4 e = *reinterpret_cast<const float4*>(stg + ((s * MU + 2) * 32) * 16);
+        h[4] = e.x; h[5] = e.y;
+        l[4] = e.z; l[5] = e.w;
+    }
+}
+
 // One strip: cells [r0, r1) along the sweep of lines [b_org, b_org + 32) of
 // instance g.inst ("row" below means a position along the sweep).
 template <int MODEL, int DIR>
@@ -152,6 +171,19 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
     const int r1 = min(r0 + A.rows, ny);
     // the x sweep reads the current buffer, the y sweep the x sweep's output
     const int bin = DIR == DIR_X ? g.cur : g.cur ^ 1, bout = bin ^ 1;
+    // Euler holds the planes in registers (2 % faster); Allaire, at its
+    // 128-register limit, spilled that way and measured 3 % slower, so it
+    // reads them from the member descriptor where it uses them
+    const MPlanes qin_r = mplanes<MODEL>(I, bin), qout_r = mplanes<MODEL>(I, bout);
+    auto qin = [&] {
+        if constexpr (MODEL == MODEL_EULER) return qin_r;
+        else return mplanes<MODEL>(I, bin);
+    };
+    auto qout = [&] {
+        if constexpr (MODEL == MODEL_EULER) return qout_r;
+        else return mplanes<MODEL>(I, bout);
+    };
+    const long long pitch = I.pitch;
     const int wall_bit = DIR == DIR_X ? 5 : 7;  // walls L, R / B, T
     const bool wall_lo = (P.flags >> wall_bit) & 1, wall_hi = (P.flags >> (wall_bit + 1)) & 1;
     const bool god = P.godunov();
@@ -188,26 +220,9 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
                 16 * lane;
     auto issue = [&](int s, int k) {
         bool ng;
-        const long long off = (long long)src_row(k, ng) * I.pitch + c;
-        cp_async16(stg + ((s * MU + 0) * 32) * 16, I.q4[bin][0] + off);
-        cp_async16(stg + ((s * MU + 1) * 32) * 16, I.q4[bin][1] + off);
-        if constexpr (MODEL == MODEL_ALLAIRE) {
-            cp_async8(stg + ((s * MU + 2) * 32) * 16, I.q2[bin][0] + off);
-            cp_async8(stg + ((s * MU + 2) * 32) * 16 + 8, I.q2[bin][1] + off);
-        }
+        mstage_issue<MODEL>(stg, s, qin(), (long long)src_row(k, ng) * pitch + c);
     };
-    // the raw cell staged in slot s (as stored: no mirror, no rotation)
-    auto staged = [&](int s, float* h, float* l) {
-        const float4 a = *reinterpret_cast<const float4*>(stg + ((s * MU + 0) * 32) * 16);
-        const float4 b = *reinterpret_cast<const float4*>(stg + ((s * MU + 1) * 32) * 16);
-        h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w;
-        l[0] = b.x; l[1] = b.y; l[2] = b.z; l[3] = b.w;
-        if constexpr (MODEL == MODEL_ALLAIRE) {
-            const float4 e = *reinterpret_cast<const float4*>(stg + ((s * MU + 2) * 32) * 16);
-            h[4] = e.x; h[5] = e.y;
-            l[4] = e.z; l[5] = e.w;
-        }
-    };
+    auto staged = [&](int s, float* h, float* l) { mstage_read<MODEL>(stg, s, h, l); };
 #pragma unroll
     for (int j = 0; j < kMAhead; ++j) {
         if (r0 - 2 + j <= r1 + 1) issue(j, r0 - 2 + j);
@@ -284,9 +299,7 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
                 else
                     dz = -k_upd * ((usR * zsR - usL * zsL) - z * (usR - usL));
                 comp_add(hh[5], ll[5], dz);
-                float zlo = (float)I.z_min, zhi = (float)(1.0 - I.z_min);
-                if (hh[5] + ll[5] < zlo) { hh[5] = zlo; ll[5] = (float)(I.z_min - (double)zlo); }
-                if (hh[5] + ll[5] > zhi) { hh[5] = zhi; ll[5] = (float)((1.0 - I.z_min) - (double)zhi); }
+                clip_z(I, hh[5], ll[5]);
                 if (hh[0] < 0.0f) { hh[0] = 0.0f; ll[0] = 0.0f; }
                 if (hh[1] < 0.0f) { hh[1] = 0.0f; ll[1] = 0.0f; }
             }
@@ -303,7 +316,8 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
                 // density / energy restore as in the plain form (rare)
                 if (!(hh[0] > 1e-12f) || !(Wn[3] + P.gp1 > 0.0f)) {
                     float oh[NV], ol[NV], Wo[NV];  // the cell before the update
-                    march_load<MODEL, DIR>(I, bin, row, c, oh, ol);
+                    load_cell<MODEL>(qin(), DIR == DIR_Y ? (long long)row * pitch + c : (long long)c * pitch + row,
+                                     oh, ol);
                     c2p_mixed<MODEL>(I, P, oh, ol, Wo);  // stored (unrotated) frame
                     float rho = hh[0] > 1e-12f ? hh[0] : oh[0];
                     float u = Wn[1], v = Wn[2];
@@ -317,9 +331,9 @@ __device__ __forceinline__ void march_strip(const MixedArgs& A, const TileGeom& 
                 }
             }
             if (live) {
-                store_cell<MODEL>(I, bout,
-                                  DIR == DIR_Y ? (long long)row * I.pitch + c
-                                               : (long long)c * I.pitch + row,
+                store_cell<MODEL>(qout(),
+                                  DIR == DIR_Y ? (long long)row * pitch + c
+                                               : (long long)c * pitch + row,
                                   hh, ll);
             }
             if (DIR == DIR_Y && live) {
@@ -393,8 +407,24 @@ __global__ void __launch_bounds__(128) mixed_march_kernel(MixedArgs A) {
 // the 32 lanes hold 32 consecutive cells of a row (kSegCells outputs plus a
 // 2-cell halo at each end), so every load and store is coalesced, and the
 // neighbours each stencil step needs (primitive states, face states, fluxes)
-// come from the adjacent lanes by warp shuffles: no shared memory, no
-// barrier.  The arithmetic is the tiled sweep's, in the same order.
+// come from the adjacent lanes by warp shuffles: no barrier, and shared
+// memory only for the rows staged ahead.  The arithmetic is the tiled
+// sweep's, in the same order.
+// Euler's rows are staged like the marching strips' (kMAhead in flight), in
+// a ring of kSSlots slots per lane: the slot refilled at row r is the one
+// read at row r - 1 (x sweep 0.255 -> 0.241 ms at 4096^2; the kernel had
+// waited on its one-row register prefetch).  Allaire's x sweep is bound by
+// instruction issue rather than load latency, and the staging instructions
+// made it 4 % slower, so it prefetches the next row into registers.
+template <int MODEL>
+__host__ __device__ constexpr bool seg_staged() {
+    return MODEL == MODEL_EULER;
+}
+constexpr int kSSlots = kMAhead + 1;
+template <int MODEL>
+__host__ __device__ constexpr int seg_smem_bytes() {
+    return seg_staged<MODEL>() ? 4 * kSSlots * march_units<MODEL>() * 32 * 16 : 0;  // 4 warps per CTA
+}
 constexpr int kSegCells = 28;  // outputs per row segment
 // rows of a tile: chosen per launch on the host (kSegMinRows..kSegRows) so
 // that the tiles fill the resident warps
@@ -423,6 +453,8 @@ __device__ __forceinline__ void segment_tile(const MixedArgs& A, const TileGeom&
     const float k_upd = (float)(dt / I.dx);
     const int nx = g.len, ny = g.wid;
     const int bin = g.cur, bout = g.cur ^ 1;
+    const MPlanes qin = mplanes<MODEL>(I, bin), qout = mplanes<MODEL>(I, bout);
+    const long long pitch = I.pitch;
     const bool god = P.godunov();
     const int lim = P.limiter();
     // this lane's column and its mirrored source (pre_sweep's fill)
@@ -440,16 +472,40 @@ __device__ __forceinline__ void segment_tile(const MixedArgs& A, const TileGeom&
     const bool writer = lane >= 2 && lane < 2 + kSegCells && ga < nx;
     const int row_end = min(g.b_org + A.rows, ny);
 
-    float nh[NV], nl[NV];
-    load_cell<MODEL>(I, bin, (long long)g.b_org * I.pitch + src, nh, nl);
+    constexpr bool staged = seg_staged<MODEL>();
+    extern __shared__ __align__(16) char seg_stage[];
+    constexpr int MU = march_units<MODEL>();
+    char* stg = seg_stage + (threadIdx.x >> 5) * (kSSlots * MU * 32 * 16) + 16 * lane;
+    float nh[NV], nl[NV];  // the next row (unstaged form)
+    if constexpr (staged) {
+#pragma unroll
+        for (int j = 0; j < kMAhead; ++j) {
+            if (g.b_org + j < row_end)
+                mstage_issue<MODEL>(stg, j, qin, (long long)(g.b_org + j) * pitch + src);
+            cp_async_commit();
+        }
+    } else {
+        load_cell<MODEL>(qin, (long long)g.b_org * pitch + src, nh, nl);
+    }
+    int slot = 0;
     for (int row = g.b_org; row < row_end; ++row) {
         float h[NV], l[NV];
+        if constexpr (staged) {
+            asm volatile("cp.async.wait_group %0;\n" ::"n"(kMAhead - 1) : "memory");
+            mstage_read<MODEL>(stg, slot, h, l);
+            if (row + kMAhead < row_end)
+                mstage_issue<MODEL>(stg, slot == 0 ? kSSlots - 1 : slot - 1, qin,
+                                    (long long)(row + kMAhead) * pitch + src);
+            cp_async_commit();
+            slot = slot == kSSlots - 1 ? 0 : slot + 1;
+        } else {
 #pragma unroll
-        for (int q = 0; q < NV; ++q) {
-            h[q] = nh[q];
-            l[q] = nl[q];
+            for (int q = 0; q < NV; ++q) {
+                h[q] = nh[q];
+                l[q] = nl[q];
+            }
+            if (row + 1 < row_end) load_cell<MODEL>(qin, (long long)(row + 1) * pitch + src, nh, nl);
         }
-        if (row + 1 < row_end) load_cell<MODEL>(I, bin, (long long)(row + 1) * I.pitch + src, nh, nl);
         if (neg) {
             h[MT::IM] = -h[MT::IM];
             l[MT::IM] = -l[MT::IM];
@@ -516,9 +572,7 @@ __device__ __forceinline__ void segment_tile(const MixedArgs& A, const TileGeom&
             else
                 dz = -k_upd * ((usR * zsR - usL * zsL) - z * (usR - usL));
             comp_add(h[5], l[5], dz);
-            float zlo = (float)I.z_min, zhi = (float)(1.0 - I.z_min);
-            if (h[5] + l[5] < zlo) { h[5] = zlo; l[5] = (float)(I.z_min - (double)zlo); }
-            if (h[5] + l[5] > zhi) { h[5] = zhi; l[5] = (float)((1.0 - I.z_min) - (double)zhi); }
+            clip_z(I, h[5], l[5]);
             if (h[0] < 0.0f) { h[0] = 0.0f; l[0] = 0.0f; }
             if (h[1] < 0.0f) { h[1] = 0.0f; l[1] = 0.0f; }
         }
@@ -528,7 +582,7 @@ __device__ __forceinline__ void segment_tile(const MixedArgs& A, const TileGeom&
             // density / energy restore as in the plain form (rare)
             if (writer && (!(h[0] > 1e-12f) || !(Wn[3] + P.gp1 > 0.0f))) {
                 float oh[NV], ol[NV], Wo[NV];  // the cell before the update
-                load_cell<MODEL>(I, bin, (long long)row * I.pitch + src, oh, ol);
+                load_cell<MODEL>(qin, (long long)row * pitch + src, oh, ol);
                 c2p_mixed<MODEL>(I, P, oh, ol, Wo);
                 float rho = h[0] > 1e-12f ? h[0] : oh[0];
                 float u = Wn[1], v = Wn[2];
@@ -539,14 +593,14 @@ __device__ __forceinline__ void segment_tile(const MixedArgs& A, const TileGeom&
                 h[3] = (p + P.gp1) * P.i1 + 0.5f * rho * (u * u + v * v); l[3] = 0.f;
             }
         }
-        if (writer) store_cell<MODEL>(I, bout, (long long)row * I.pitch + ga, h, l);
+        if (writer) store_cell<MODEL>(qout, (long long)row * pitch + ga, h, l);
     }
 }
 
 // Persistent x sweep: warp w of the W warps of the grid walks the tiles w,
-// w + W, w + 2W, ... of the launch's tile list.  Euler: 8 CTAs per
-// SM (64 registers, 20 bytes spilled) measured 8 % faster than the 7 that
-// its unbounded 72 registers allow; Allaire is fastest unbounded.
+// w + W, w + 2W, ... of the launch's tile list.  Euler is bounded to 64
+// registers for 8 CTAs per SM (8 % faster than 7 CTAs when the next row was
+// still prefetched into registers); Allaire is fastest unbounded.
 template <int MODEL>
 __global__ void __launch_bounds__(128, MODEL == MODEL_EULER ? 8 : 1)
     mixed_segment_x_kernel(MixedArgs A) {

@@ -153,7 +153,7 @@ __device__ __forceinline__ void c2p_mixed(const Inst& I, const MPar& P, const fl
             double M1 = (double)hi[1] + (double)lo[1], M2 = (double)hi[2] + (double)lo[2];
             double E = (double)hi[3] + (double)lo[3];
             double re = E - 0.5 * (M1 * M1 + M2 * M2) / R;
-            p = (float)(I.eos.gm1_1 * re - I.eos.gp1);
+            p = (float)(__ldg(&I.eos.gm1_1) * re - __ldg(&I.eos.gp1));
         }
         W[0] = rho;
         W[1] = u;
@@ -178,8 +178,8 @@ __device__ __forceinline__ void c2p_mixed(const Inst& I, const MPar& P, const fl
             double E = (double)hi[4] + (double)lo[4];
             double zz = (double)hi[5] + (double)lo[5];
             double omz = 1.0 - zz;
-            double eps = zz * I.pd[0] + omz * I.pd[1];
-            double kn = zz * I.pd[2] + omz * I.pd[3];
+            double eps = zz * __ldg(I.pd + 0) + omz * __ldg(I.pd + 1);
+            double kn = zz * __ldg(I.pd + 2) + omz * __ldg(I.pd + 3);
             p = fdiv((float)((E * R - 0.5 * (M1 * M1 + M2 * M2)) - kn * R), (float)(R * eps));
         }
         W[0] = hi[0];
@@ -386,27 +386,65 @@ __device__ __forceinline__ void comp_add(float& hi, float& lo, float d) {
     lo = e;
 }
 
-template <int MODEL> __device__ __forceinline__ void load_cell(const Inst& I, int buf,
-                                                               long long off, float* h, float* l) {
-    float4 a = __ldg(I.q4[buf][0] + off), b = __ldg(I.q4[buf][1] + off);
+// The planes of one state buffer of a member, held in registers: the stores
+// of a sweep go through pointers the compiler cannot tell apart from the
+// member descriptor, so reading the descriptor's pointers again after every
+// store would cost a global load each time.
+struct MPlanes {
+    float4 *v4, *c4;  // components 0-3: value, compensation
+    float2 *v2, *c2;  // Allaire E, z: value, compensation
+};
+
+template <int MODEL>
+__device__ __forceinline__ MPlanes mplanes(const Inst& I, int buf) {
+    MPlanes q;
+    q.v4 = I.q4[buf][0];
+    q.c4 = I.q4[buf][1];
+    q.v2 = MODEL == MODEL_ALLAIRE ? I.q2[buf][0] : nullptr;
+    q.c2 = MODEL == MODEL_ALLAIRE ? I.q2[buf][1] : nullptr;
+    return q;
+}
+
+template <int MODEL> __device__ __forceinline__ void load_cell(const MPlanes& Q, long long off, float* h,
+                                                               float* l) {
+    float4 a = __ldg(Q.v4 + off), b = __ldg(Q.c4 + off);
     h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w;
     l[0] = b.x; l[1] = b.y; l[2] = b.z; l[3] = b.w;
     if constexpr (MODEL == MODEL_ALLAIRE) {
-        float2 c = __ldg(I.q2[buf][0] + off), d = __ldg(I.q2[buf][1] + off);
+        float2 c = __ldg(Q.v2 + off), d = __ldg(Q.c2 + off);
         h[4] = c.x; h[5] = c.y;
         l[4] = d.x; l[5] = d.y;
     }
 }
 
+template <int MODEL> __device__ __forceinline__ void store_cell(const MPlanes& Q, long long off,
+                                                                const float* h, const float* l) {
+    Q.v4[off] = make_float4(h[0], h[1], h[2], h[3]);
+    Q.c4[off] = make_float4(l[0], l[1], l[2], l[3]);
+    if constexpr (MODEL == MODEL_ALLAIRE) {
+        Q.v2[off] = make_float2(h[4], h[5]);
+        Q.c2[off] = make_float2(l[4], l[5]);
+    }
+}
+
+template <int MODEL> __device__ __forceinline__ void load_cell(const Inst& I, int buf,
+                                                               long long off, float* h, float* l) {
+    load_cell<MODEL>(mplanes<MODEL>(I, buf), off, h, l);
+}
+
+// The clip of the updated volume fraction to [z_min, 1 - z_min] on a
+// compensated z (value h, compensation l).
+__device__ __forceinline__ void clip_z(const Inst& I, float& h, float& l) {
+    const double zm = __ldg(&I.z_min);
+    const float zlo = (float)zm, zhi = (float)(1.0 - zm);
+    if (h + l < zlo) { h = zlo; l = (float)(zm - (double)zlo); }
+    if (h + l > zhi) { h = zhi; l = (float)((1.0 - zm) - (double)zhi); }
+}
+
 template <int MODEL> __device__ __forceinline__ void store_cell(const Inst& I, int buf,
                                                                 long long off, const float* h,
                                                                 const float* l) {
-    I.q4[buf][0][off] = make_float4(h[0], h[1], h[2], h[3]);
-    I.q4[buf][1][off] = make_float4(l[0], l[1], l[2], l[3]);
-    if constexpr (MODEL == MODEL_ALLAIRE) {
-        I.q2[buf][0][off] = make_float2(h[4], h[5]);
-        I.q2[buf][1][off] = make_float2(l[4], l[5]);
-    }
+    store_cell<MODEL>(mplanes<MODEL>(I, buf), off, h, l);
 }
 
 // Shared-memory vectors: one float4 (+ one float2 for Allaire) per slot.
@@ -688,9 +726,7 @@ __device__ __forceinline__ void mixed_tile(const MixedArgs& A, const TileGeom& g
                     dz = -k_upd * ((usR * zsR - usL * zsL) - z * (usR - usL));
                 }
                 comp_add(hh[5], ll[5], dz);
-                float zlo = (float)I.z_min, zhi = (float)(1.0 - I.z_min);
-                if (hh[5] + ll[5] < zlo) { hh[5] = zlo; ll[5] = (float)(I.z_min - (double)zlo); }
-                if (hh[5] + ll[5] > zhi) { hh[5] = zhi; ll[5] = (float)((1.0 - I.z_min) - (double)zhi); }
+                clip_z(I, hh[5], ll[5]);
                 if (hh[0] < 0.0f) { hh[0] = 0.0f; ll[0] = 0.0f; }
                 if (hh[1] < 0.0f) { hh[1] = 0.0f; ll[1] = 0.0f; }
             }
