@@ -103,12 +103,12 @@ __device__ __forceinline__ void march_finish(DevState* st, const double* partial
 // while row k is computed; kMAhead rows in flight, row k + kMAhead issued
 // into the slot of row k - 3 once row k has arrived; per slot MU 16-byte
 // units per lane (value and compensation words of components 0-3; for
-// Allaire E and z with their compensation words).  The raw cells of rows
-// k-1 and k-2 that the update of row k-2 starts from are therefore read
-// again from the ring rather than carried in registers: 124 -> 115
-// registers for Euler and 5 % less time per y sweep; Allaire's carried
-// window (face state, flux) then fits in its 128 registers, where it had
-// to sit in shared memory before.
+// Allaire E and z with their compensation words).  The raw cells of row
+// k-2, which its update starts from, are therefore read again from the
+// ring rather than carried in registers for two rows: 124 -> 115 registers
+// for Euler and 5 % less time per y sweep; Allaire's carried window (face
+// state, flux) then fits in its 128 registers, where it had to sit in
+// shared memory before.
 constexpr int kMAhead = 3, kMSlots = kMAhead + 3;
 template <int MODEL>
 __host__ __device__ constexpr int march_units() {
@@ -121,8 +121,8 @@ __host__ __device__ constexpr int march_smem_bytes() {
     return 4 * kMSlots * march_units<MODEL>() * 32 * 16;
 }
 
-// Starts copying the cell at element offset `off` of buffer `buf` (value and
-// compensation words) into slot `s` of this lane's staging ring `stg`.
+// Starts copying the cell at element offset `off` of the planes `Q` (value
+// and compensation words) into slot `s` of this lane's staging ring `stg`.
 template <int MODEL>
 __device__ __forceinline__ void mstage_issue(char* stg, int s, const MPlanes& Q, long long off) {
     constexpr int MU = march_units<MODEL>();
