@@ -191,17 +191,22 @@ __device__ __forceinline__ void c2p_mixed(const Inst& I, const MPar& P, const fl
     }
 }
 
-// Physical primitive state: the conversion to conserved variables would give
-// rho >= 0 and e >= 0 (and 0 <= z <= 1, partial densities >= 0).
+// Physical primitive state: the reference's test on the conserved state
+// (E/headers/misc_euler.hpp:123-131, A/headers/misc.hpp:228-237) passes,
+// i.e. rho >= 0 and e >= 0 (and 0 <= z <= 1, partial densities >= 0).  Its
+// e is computed with divisions by rho, so a zero density gives e = NaN and
+// fails the test: the density must be strictly positive (a face state of
+// zero density taken as physical produced infinite sound speeds and NaN
+// fluxes on unlimited slopes at a contact).
 template <int MODEL> __device__ __forceinline__ bool phys_prim(const MPar& P, const float* W) {
     if constexpr (MODEL == MODEL_EULER) {
-        return W[0] >= 0.0f && W[3] + P.gp1 >= 0.0f;
+        return W[0] > 0.0f && W[3] + P.gp1 >= 0.0f;
     } else {
         // p + k >= 0  <=>  p eps + kn >= 0 (eps > 0 for 0 <= z <= 1)
         float omz = 1.0f - W[5];
         float eps = W[5] * P.i1 + omz * P.i2, kn = W[5] * P.c1 + omz * P.c2;
-        return W[0] >= 0.0f && W[1] >= 0.0f && W[5] >= 0.0f && W[5] <= 1.0f &&
-               W[4] * eps + kn >= 0.0f;
+        return W[0] >= 0.0f && W[1] >= 0.0f && W[0] + W[1] > 0.0f && W[5] >= 0.0f &&
+               W[5] <= 1.0f && W[4] * eps + kn >= 0.0f;
     }
 }
 
