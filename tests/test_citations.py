@@ -51,11 +51,12 @@ def test_cited_line_ranges_exist():
     r = subprocess.run(["git", "ls-files"], cwd=ROOT, capture_output=True, text=True)
     if r.returncode == 0:
         files = r.stdout.split()
-    else:  # a copy without git history: every file outside the scratch and build trees
-        skip = ("_work/", "gpurun_out/", "baseline/", "oracle/_ref/", "oracle/_build/",
-                "cfd-art_b200/lib/")
-        files = [str(p.relative_to(ROOT)) for p in ROOT.rglob("*") if p.is_file()]
-        files = [f for f in files if not f.startswith(skip) and "/." not in "/" + f]
+    else:  # a copy without git history: the source trees, without their build outputs
+        trees = ("cfd-art_b200", "include", "oracle", "tests", "profiles")
+        files = [str(p.relative_to(ROOT)) for t in trees for p in (ROOT / t).rglob("*") if p.is_file()]
+        files += [p.name for p in ROOT.glob("*.py")]
+        build = ("cfd-art_b200/lib/", "oracle/_ref/", "oracle/_build/")
+        files = [f for f in files if not f.startswith(build) and "/." not in "/" + f]
     bad = []
     for f in files:
         source = f.endswith((".py", ".cu", ".cuh", ".h", ".cpp", ".c", ".hpp"))
