@@ -604,9 +604,17 @@ class Server:
         self.cfgs[rid.value] = cfg.copy()
         return rid.value
 
-    def wait(self, rid: int, timeout: float = -1.0, want_result: bool = True):
+    def wait(self, rid: int, timeout: float = -1.0, want_result: bool = True,
+             out: np.ndarray | None = None):
+        """Waits for request `rid`; returns its info and its final grid (into
+        `out` when given: a C-contiguous float64 array of the ghosted shape)."""
         info = RequestInfo()
-        out = np.empty(self.cfgs[rid].ghosted_shape()) if want_result else None
+        if out is not None:
+            shape = self.cfgs[rid].ghosted_shape()
+            if out.shape != tuple(shape) or out.dtype != np.float64 or not out.flags.c_contiguous:
+                raise ValueError(f"out must be a C-contiguous float64 array of shape {tuple(shape)}")
+        elif want_result:
+            out = np.empty(self.cfgs[rid].ghosted_shape())
         check(lib().cfd_server_wait(self._h, rid, timeout, C.byref(info),
                                     _dp(out) if out is not None else None), "cfd_server_wait")
         return info, out
