@@ -43,6 +43,24 @@ def test_served_in_mix_equals_served_alone(precision):
         assert np.array_equal(out1, out)
 
 
+def test_wait_into_the_clients_buffer():
+    """A result lands in the buffer the client passes (the same bits as a
+    fresh array); a buffer of the wrong shape or type is refused before
+    the call."""
+    c, ic, n = _requests()[1]
+    with G.Server(G.MIXED, ticks_per_round=8) as srv:
+        a, b = srv.submit(c, ic, n), srv.submit(c, ic, n)
+        with pytest.raises(ValueError):
+            srv.wait(a, out=np.empty((3, 3, c.nvar)))
+        with pytest.raises(ValueError):
+            srv.wait(a, out=np.empty(c.ghosted_shape(), dtype=np.float32))
+        buf = np.full(c.ghosted_shape(), np.nan)
+        info, got = srv.wait(a, out=buf)
+        _, fresh = srv.wait(b)
+    assert got is buf and info.steps == n
+    assert np.array_equal(buf, fresh)
+
+
 def test_fp64_served_equals_solver():
     c, ic, n = _requests()[0]
     with G.Server(G.FP64, ticks_per_round=16) as srv:
