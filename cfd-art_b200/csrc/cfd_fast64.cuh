@@ -856,8 +856,8 @@ __device__ __forceinline__ void segment64_tile(const MixedArgs& A, const TileGeo
             }
             hllc<MODEL>(P, WL, WR, F);
         }
-        double FR[NV + 2];
-        shfl_down64<NV + 2>(F, FR);
+        double FR[NV + 2];  // Euler's update needs only the NV fluxes, not u*
+        shfl_down64<MODEL == MODEL_EULER ? NV : NV + 2>(F, FR);
 
         // update (lanes 2 .. 2 + kSegCells - 1)
         double N[NV];

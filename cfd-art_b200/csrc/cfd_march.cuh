@@ -554,8 +554,8 @@ __device__ __forceinline__ void segment_tile(const MixedArgs& A, const TileGeom&
             }
             hllc_prim<MODEL>(P, WL, WR, F);
         }
-        float FR[NV + 2];
-        shfl_down_n<NV + 2>(F, FR);
+        float FR[NV + 2];  // Euler's update needs only the NV fluxes, not u*
+        shfl_down_n<MODEL == MODEL_EULER ? NV : NV + 2>(F, FR);
 
         // compensated update (lanes 2 .. 2 + kSegCells - 1)
 #pragma unroll
